@@ -1,0 +1,122 @@
+/* dtwj — top-1 z-normalised DTW subsequence self-join on one NVIDIA B200.
+ *
+ * C ABI of libdtwj.so.  Plain pointers and sizes; no C++ or framework types.
+ *
+ * The reference (QW1k0YA/Scaling-Subsequence-Similarity-Join-Based-on-Dynamic-
+ * Time-Warping-CPU-GPU) ships two executables and no library; its in-process
+ * seam for this path is
+ *     void DTWMotifDiscoveryGUI(const vector<T>& TS, int subseqlen, int maxwarp,
+ *                               const char* output_time_file_path)
+ * (CPU_version1/DTWMotifDiscoveryGUI.cpp:12, GPU_version1/src/DTWMotifDiscoveryGUI.cu:12),
+ * which runs mpx_v2 and then new_dtw_motifGUI[_malloc]
+ * (CPU_version1/new_dtw_motifGUI.cpp:21, GPU_version1/src/new_dtw_motifGUI_malloc.cu:30)
+ * and prints the result.  dtwj_join() replaces that seam and returns the
+ * result instead of printing it; the `dtwj` CLI replaces the executables'
+ * argv interface (README.md:15-34, GPU_version1/src/AAAA.cu:17-36).
+ *
+ * Semantics shared by every entry point:
+ *   n series length, m subsequence length, w Sakoe-Chiba band (cells with
+ *   |r - c| <= w), s = n - m + 1 subsequences, each z-normalised with its own
+ *   mean and population standard deviation.  Candidate pairs are (i, j) with
+ *   j - i >= m (the reference's exclusion zone, minlag = m,
+ *   CPU_version1/new_dtw_motifGUI.cpp:182).  Windows with zero deviation are
+ *   excluded.  Indices are 0-based.  The top-1 pair minimises
+ *   (dist, i, j) lexicographically, so exact ties go to the lowest index.
+ *
+ * Errors: every function returns DTWJ_OK (0) or a negative DTWJ_ERR_* code;
+ * dtwj_strerror() names it.  Nothing calls exit().  Inputs are read-only and
+ * owned by the caller; the library owns all device memory it allocates.
+ * Calls on one dtwj_ctx must not overlap; distinct contexts may be used from
+ * distinct host threads.
+ */
+#ifndef DTWJ_H
+#define DTWJ_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DTWJ_OK 0
+#define DTWJ_ERR_ARG (-1)       /* invalid n, m, w, pointer or flags          */
+#define DTWJ_ERR_NAN (-2)       /* input contains NaN or infinity             */
+#define DTWJ_ERR_CUDA (-3)      /* a CUDA call failed                         */
+#define DTWJ_ERR_OOM (-4)       /* device allocation failed                   */
+#define DTWJ_ERR_BAND (-5)      /* 2w+1 exceeds the register band (w <= 255)  */
+#define DTWJ_ERR_OVERFLOW (-6)  /* candidate list overflowed                  */
+#define DTWJ_ERR_TIMEOUT (-7)   /* a bounded device-side wait ran out         */
+#define DTWJ_ERR_NODEVICE (-8)  /* no CUDA device                             */
+#define DTWJ_ERR_IO (-9)        /* file could not be read or written          */
+#define DTWJ_ERR_NOMODEL (-10)  /* learned ordering requested, no model loaded */
+
+/* flags */
+#define DTWJ_F_NO_MASKED 0x1u   /* skip the masked diagonal bound             */
+#define DTWJ_F_NO_SEED 0x2u     /* no ED-profile seeding of the best-so-far   */
+#define DTWJ_F_NO_DIAG 0x4u     /* skip all diagonal bounds (LB_Keogh + DTW)  */
+#define DTWJ_F_LEARNED 0x8u     /* order the tile queue with the loaded MLP   */
+#define DTWJ_F_VERBOSE 0x10u    /* phase timings on stderr                    */
+
+typedef struct {
+  int64_t i, j;            /* top-1 pair, 0-based, j - i >= m                */
+  double dist;             /* its DTW distance, recomputed in FP64           */
+  double dist_fp32;        /* the FP32 distance the device search found      */
+  double seed_bsf;         /* best-so-far after the ED-profile seeds         */
+  uint64_t pairs;          /* candidate pairs (non-flat, j - i >= m)         */
+  uint64_t pruned_fast;    /* pruned by the O(1) diagonal ED/LB_Keogh bound  */
+  uint64_t pruned_kim;     /* pruned by the endpoint bound                   */
+  uint64_t pruned_masked;  /* pruned by the masked diagonal bound            */
+  uint64_t pruned_keogh;   /* pruned by LB_Keogh (either direction)          */
+  uint64_t dtw_calls;      /* banded DTW evaluations (FP32)                  */
+  uint64_t dtw_abandoned;  /* of which abandoned early                       */
+  uint64_t dtw_cells;      /* DTW cells swept                                */
+  uint64_t candidates;     /* pairs re-verified in FP64                      */
+  double seconds_join;     /* device time of the join, inputs resident       */
+  double seconds_total;    /* wall time of the call                          */
+  int64_t n;
+  int32_t m, w;
+} dtwj_result;
+
+typedef struct dtwj_ctx dtwj_ctx;
+
+/* One-shot join of a host series (DTWMotifDiscoveryGUI's seam). */
+int dtwj_join(const double* x, int64_t n, int32_t m, int32_t w, uint32_t flags,
+              dtwj_result* out);
+
+/* Many independent series, each with its own m and w; outs[k] is identical to
+ * dtwj_join(xs[k], ns[k], ms[k], ws[k], flags).  No reference counterpart
+ * (the reference joins one series per process). */
+int dtwj_join_batch(const double* const* xs, const int64_t* ns, const int32_t* ms,
+                    const int32_t* ws, int32_t count, uint32_t flags, dtwj_result* outs);
+
+/* Reusable context bound to one device: keeps device buffers between calls. */
+int dtwj_ctx_create(int device, dtwj_ctx** out);
+void dtwj_ctx_destroy(dtwj_ctx* ctx);
+int dtwj_ctx_join(dtwj_ctx* ctx, const double* x_host, int64_t n, int32_t m, int32_t w,
+                  uint32_t flags, dtwj_result* out);
+/* Same, with the series already in device memory (x_dev: n doubles). */
+int dtwj_ctx_join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m,
+                         int32_t w, uint32_t flags, dtwj_result* out);
+
+/* z-normalised Euclidean matrix profile with exclusion zone m (mpx_v2,
+ * CPU_version1/mpx_v2.cpp:13): mp[i] = min over |i-j| >= m, mpi[i] its
+ * 0-based argmin (lowest index on ties; -1 and +inf when none).  mp, mpi
+ * hold s = n - m + 1 entries. */
+int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64_t* mpi);
+
+/* Banded DTW distances of explicit pairs of subsequences of x (the exact
+ * recurrence MON_dtw computes, CPU_version1/MON_DTW.cpp:20), FP32 on the
+ * device (precise=0) or FP64 (precise=1).  dist[k] for (pi[k], pj[k]). */
+int dtwj_pair_dtw(const double* x, int64_t n, int32_t m, int32_t w, const int64_t* pi,
+                  const int64_t* pj, int64_t count, int32_t precise, double* dist);
+
+/* Band from a ratio: ceil(ratio*m) (rounding=0) or the reference's
+ * max(round(ratio*m), 1) (rounding=1, GPU_version1/src/AAAA.cu:34). */
+int32_t dtwj_band(int32_t m, double ratio, int32_t rounding);
+
+const char* dtwj_strerror(int code);
+int dtwj_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,144 @@
+// Test infrastructure only (the oracle): a C ABI around the reference's own
+// FP64 CPU implementation (CPU_version1), linked from objects that
+// oracle/build_ref.sh compiles out of the reference tree.  Tests, smoke() and
+// bench.py's CPU-baseline leg call it through ctypes as the checker; the
+// product never links it.
+//
+// Every function here forwards to the reference function it names:
+//   ref_join      -> DTWMotifDiscoveryGUI   CPU_version1/DTWMotifDiscoveryGUI.cpp:12
+//                    (mpx_v2 + new_dtw_motifGUI, CPU_version1/new_dtw_motifGUI.cpp:21)
+//   ref_mon_dtw   -> MON_dtw                CPU_version1/MON_DTW.cpp:20
+//   ref_mvmean    -> mvmean                 CPU_version1/allmatrixop/movmean.cpp:9
+//   ref_lemire    -> lower_upper_lemire     CPU_version1/allmatrixop/lower_upper_lemire.cpp:7
+//   ref_mpx       -> mpx_v2                 CPU_version1/mpx_v2.cpp:13
+#include "alldef/matrix.h"
+#include "alldef/allstruct.h"
+#include "allunder/underdtw.h"
+#include <unistd.h>
+#include <fcntl.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <chrono>
+
+RETURN_MPX mpx_v2(const vector<DOUBLE>& timeSeries, int minlag, int subseqlen);
+void DTWMotifDiscoveryGUI(const vector<DOUBLE>& TS, int subseqlen, int maxwarp,
+                          const char* output_time_file_path);
+
+namespace {
+
+// Runs fn() with file descriptor 1 pointed at a temporary file and returns
+// everything the reference printed.
+template <class F>
+std::string capture_stdout(F fn) {
+  fflush(stdout);
+  std::cout.flush();
+  char path[] = "/tmp/dtwj_ref_XXXXXX";
+  int fd = mkstemp(path);
+  if (fd < 0) { fn(); return std::string(); }
+  int saved = dup(1);
+  dup2(fd, 1);
+  fn();
+  fflush(stdout);
+  std::cout.flush();
+  dup2(saved, 1);
+  close(saved);
+  std::string out;
+  lseek(fd, 0, SEEK_SET);
+  char buf[65536];
+  ssize_t k;
+  while ((k = read(fd, buf, sizeof buf)) > 0) out.append(buf, (size_t)k);
+  close(fd);
+  unlink(path);
+  return out;
+}
+
+bool find_double_after(const std::string& s, const char* key, double* v) {
+  size_t p = s.rfind(key);
+  if (p == std::string::npos) return false;
+  return sscanf(s.c_str() + p + strlen(key), "%lf", v) == 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Squared banded DTW of two equal-length sequences with no early abandoning
+// (cumulative bound all zeros, best-so-far effectively infinite).
+double ref_mon_dtw(const double* q, const double* t, int m, int w) {
+  std::vector<double> a(q, q + m), b(t, t + m), cb((size_t)m + w + 2, 0.0);
+  return MON_dtw(a, b, cb, m, w, 1e300);
+}
+
+void ref_mvmean(const double* a, long n, int m, double* mu, double* sig) {
+  std::vector<double> v(a, a + n);
+  long s = n - m + 1;
+  std::vector<double> mv(s), sv(s);
+  mvmean(v, m, mv, sv);
+  for (long i = 0; i < s; ++i) { mu[i] = mv[i]; sig[i] = sv[i]; }
+}
+
+void ref_lemire(const double* a, int n, int r, double* lower, double* upper) {
+  std::vector<double> v(a, a + n), l(n), u(n);
+  lower_upper_lemire(v, n, r, l, u);
+  for (int i = 0; i < n; ++i) { lower[i] = l[i]; upper[i] = u[i]; }
+}
+
+// ED matrix profile with exclusion zone m: mp = z-normalised Euclidean
+// distance, mpi = 1-based index of the nearest neighbour (reference layout).
+void ref_mpx(const double* a, long n, int m, double* mp, int* mpi) {
+  std::vector<double> v(a, a + n);
+  RETURN_MPX r;
+  capture_stdout([&] { r = mpx_v2(v, m, m); });
+  for (size_t i = 0; i < r.matrixProfile.size(); ++i) {
+    mp[i] = r.matrixProfile[i];
+    mpi[i] = r.matrixProfileIdx[i];
+  }
+}
+
+// One full reference join (mpx_v2 + new_dtw_motifGUI).  Outputs 0-based pair
+// indices, the distance as printed (%f), the distance recomputed at full FP64
+// precision with the reference's own z-normalisation and MON_dtw, the
+// reference's own join time (clock() t1->t2) and the wall time of the call.
+// Returns 0 on success, 1 if the reference's output could not be parsed.
+int ref_join(const double* x, long n, int m, int w, const char* timefile,
+             long long* i_out, long long* j_out, double* dist_printed,
+             double* dist_full, double* join_seconds, double* wall_seconds) {
+  std::vector<double> ts(x, x + n);
+  auto t0 = std::chrono::steady_clock::now();
+  std::string out = capture_stdout([&] { DTWMotifDiscoveryGUI(ts, m, w, timefile); });
+  auto t1 = std::chrono::steady_clock::now();
+  *wall_seconds = std::chrono::duration<double>(t1 - t0).count();
+  double fm = 0, sm = 0, dist = 0, secs = 0;
+  size_t p = out.rfind("first min is ");
+  if (p == std::string::npos ||
+      sscanf(out.c_str() + p, "first min is %lf sec min is %lf", &fm, &sm) != 2)
+    return 1;
+  if (!find_double_after(out, "final distance :", &dist)) return 1;
+  if (!find_double_after(out, "total time is ", &secs)) secs = -1;
+  long long i0 = (long long)llround(fm) - 1, j0 = (long long)llround(sm) - 1;
+  *i_out = i0;
+  *j_out = j0;
+  *dist_printed = dist;
+  *join_seconds = secs;
+  // Full-precision distance of the reported pair, z-normalised exactly as
+  // new_dtw_motifGUI does ((a - mu) / sig with mvmean's statistics).
+  long s = n - m + 1;
+  std::vector<double> mu(s), sig(s);
+  mvmean(ts, m, mu, sig);
+  *dist_full = NAN;
+  if (i0 >= 0 && j0 >= 0 && i0 < s && j0 < s) {
+    std::vector<double> q(m), t(m), cb((size_t)m + w + 2, 0.0);
+    for (int k = 0; k < m; ++k) {
+      q[k] = (ts[i0 + k] - mu[i0]) / sig[i0];
+      t[k] = (ts[j0 + k] - mu[j0]) / sig[j0];
+    }
+    *dist_full = std::sqrt(MON_dtw(q, t, cb, m, w, 1e300));
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,278 @@
+"""dtwj: B200-native top-1 z-normalised DTW subsequence self-join.
+
+Python binding over the C ABI of lib/libdtwj.so (include/dtwj.h).  The
+library is the product; this module only marshals arrays.  Loading fails
+loudly when the shared library is missing: there is no CPU fallback.
+
+Reference seam mirrored here: ``DTWMotifDiscoveryGUI(TS, subseqlen, maxwarp,
+output_time_file_path)`` (CPU_version1/DTWMotifDiscoveryGUI.cpp:12) runs the
+ED matrix profile and the join, prints the result and appends the join time
+to the file; :func:`dtw_motif_discovery` does the same and also returns the
+result.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libdtwj.so")
+CLI_PATH = os.path.join(_HERE, "bin", "dtwj")
+
+OK = 0
+ERR_ARG = -1
+ERR_NAN = -2
+ERR_CUDA = -3
+ERR_OOM = -4
+ERR_BAND = -5
+ERR_OVERFLOW = -6
+ERR_TIMEOUT = -7
+ERR_NODEVICE = -8
+ERR_IO = -9
+ERR_NOMODEL = -10
+
+F_NO_MASKED = 0x1
+F_NO_SEED = 0x2
+F_NO_DIAG = 0x4
+F_LEARNED = 0x8
+F_VERBOSE = 0x10
+
+# Every symbol include/dtwj.h declares.
+EXPORTS = (
+    "dtwj_join",
+    "dtwj_join_batch",
+    "dtwj_ctx_create",
+    "dtwj_ctx_destroy",
+    "dtwj_ctx_join",
+    "dtwj_ctx_join_device",
+    "dtwj_matrix_profile",
+    "dtwj_pair_dtw",
+    "dtwj_band",
+    "dtwj_strerror",
+    "dtwj_device_count",
+)
+
+
+class DtwjError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        super().__init__("%s%s (code %d)" % (what + ": " if what else "", strerror(code), code))
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [
+        ("i", ctypes.c_int64),
+        ("j", ctypes.c_int64),
+        ("dist", ctypes.c_double),
+        ("dist_fp32", ctypes.c_double),
+        ("seed_bsf", ctypes.c_double),
+        ("pairs", ctypes.c_uint64),
+        ("pruned_fast", ctypes.c_uint64),
+        ("pruned_kim", ctypes.c_uint64),
+        ("pruned_masked", ctypes.c_uint64),
+        ("pruned_keogh", ctypes.c_uint64),
+        ("dtw_calls", ctypes.c_uint64),
+        ("dtw_abandoned", ctypes.c_uint64),
+        ("dtw_cells", ctypes.c_uint64),
+        ("candidates", ctypes.c_uint64),
+        ("seconds_join", ctypes.c_double),
+        ("seconds_total", ctypes.c_double),
+        ("n", ctypes.c_int64),
+        ("m", ctypes.c_int32),
+        ("w", ctypes.c_int32),
+    ]
+
+
+@dataclass
+class JoinResult:
+    i: int
+    j: int
+    dist: float
+    dist_fp32: float
+    seed_bsf: float
+    pairs: int
+    pruned_fast: int
+    pruned_kim: int
+    pruned_masked: int
+    pruned_keogh: int
+    dtw_calls: int
+    dtw_abandoned: int
+    dtw_cells: int
+    candidates: int
+    seconds_join: float
+    seconds_total: float
+    n: int
+    m: int
+    w: int
+
+    @staticmethod
+    def _from(r: _Result) -> "JoinResult":
+        return JoinResult(**{name: getattr(r, name) for name, _ in _Result._fields_})
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libdtwj.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError("libdtwj.so not built at %s (run build.py)" % path)
+    lib = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    d = ctypes.c_double
+    i32, i64, u32 = ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32
+    lib.dtwj_join.argtypes = [P(d), i64, i32, i32, u32, P(_Result)]
+    lib.dtwj_join_batch.argtypes = [P(P(d)), P(i64), P(i32), P(i32), i32, u32, P(_Result)]
+    lib.dtwj_ctx_create.argtypes = [ctypes.c_int, P(ctypes.c_void_p)]
+    lib.dtwj_ctx_destroy.argtypes = [ctypes.c_void_p]
+    lib.dtwj_ctx_destroy.restype = None
+    lib.dtwj_ctx_join.argtypes = [ctypes.c_void_p, P(d), i64, i32, i32, u32, P(_Result)]
+    lib.dtwj_ctx_join_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, i64, i32, i32, u32,
+                                         P(_Result)]
+    lib.dtwj_matrix_profile.argtypes = [P(d), i64, i32, P(d), P(i64)]
+    lib.dtwj_pair_dtw.argtypes = [P(d), i64, i32, i32, P(i64), P(i64), i64, i32, P(d)]
+    lib.dtwj_band.argtypes = [i32, d, i32]
+    lib.dtwj_band.restype = i32
+    lib.dtwj_strerror.argtypes = [ctypes.c_int]
+    lib.dtwj_strerror.restype = ctypes.c_char_p
+    lib.dtwj_device_count.argtypes = []
+    _lib = lib
+    return lib
+
+
+def _f64(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def strerror(code: int) -> str:
+    return load().dtwj_strerror(code).decode()
+
+
+def device_count() -> int:
+    return int(load().dtwj_device_count())
+
+
+def band(m: int, ratio: float, rounding: str = "ceil") -> int:
+    return int(load().dtwj_band(m, ratio, 1 if rounding == "round" else 0))
+
+
+def join(x, m: int, w: int, flags: int = 0) -> JoinResult:
+    """Top-1 z-normalised DTW pair of x (j - i >= m, band w)."""
+    a = _f64(x)
+    r = _Result()
+    rc = load().dtwj_join(_dptr(a), a.size, m, w, flags, ctypes.byref(r))
+    if rc != OK:
+        raise DtwjError(rc, "dtwj_join")
+    return JoinResult._from(r)
+
+
+def join_batch(series, ms, ws, flags: int = 0) -> list[JoinResult]:
+    arrs = [_f64(x) for x in series]
+    k = len(arrs)
+    ptrs = (ctypes.POINTER(ctypes.c_double) * k)(*[_dptr(a) for a in arrs])
+    ns = (ctypes.c_int64 * k)(*[a.size for a in arrs])
+    mm = (ctypes.c_int32 * k)(*ms)
+    ww = (ctypes.c_int32 * k)(*ws)
+    outs = (_Result * k)()
+    rc = load().dtwj_join_batch(ptrs, ns, mm, ww, k, flags, outs)
+    if rc != OK:
+        raise DtwjError(rc, "dtwj_join_batch")
+    return [JoinResult._from(outs[q]) for q in range(k)]
+
+
+class Context:
+    """Reusable device context (keeps device buffers between joins)."""
+
+    def __init__(self, device: int = 0):
+        lib = load()
+        h = ctypes.c_void_p()
+        rc = lib.dtwj_ctx_create(device, ctypes.byref(h))
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_create")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            load().dtwj_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def join(self, x, m: int, w: int, flags: int = 0) -> JoinResult:
+        a = _f64(x)
+        r = _Result()
+        rc = load().dtwj_ctx_join(self._h, _dptr(a), a.size, m, w, flags, ctypes.byref(r))
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_join")
+        return JoinResult._from(r)
+
+    def join_device(self, dev_ptr: int, n: int, m: int, w: int, flags: int = 0) -> JoinResult:
+        """Join a series already in device memory (dev_ptr: n float64)."""
+        r = _Result()
+        rc = load().dtwj_ctx_join_device(self._h, ctypes.c_void_p(dev_ptr), n, m, w, flags,
+                                         ctypes.byref(r))
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_join_device")
+        return JoinResult._from(r)
+
+
+def matrix_profile(x, m: int):
+    """(mp, mpi): z-normalised ED matrix profile, exclusion zone m."""
+    a = _f64(x)
+    s = a.size - m + 1
+    mp = np.empty(max(s, 0), dtype=np.float64)
+    mpi = np.empty(max(s, 0), dtype=np.int64)
+    rc = load().dtwj_matrix_profile(_dptr(a), a.size, m, _dptr(mp),
+                                    mpi.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    if rc != OK:
+        raise DtwjError(rc, "dtwj_matrix_profile")
+    return mp, mpi
+
+
+def pair_dtw(x, m: int, w: int, pi, pj, precise: bool = True) -> np.ndarray:
+    """Banded DTW distances of the z-normalised subsequence pairs (pi[k], pj[k])."""
+    a = _f64(x)
+    pi = np.ascontiguousarray(pi, dtype=np.int64)
+    pj = np.ascontiguousarray(pj, dtype=np.int64)
+    out = np.empty(pi.size, dtype=np.float64)
+    P64 = ctypes.POINTER(ctypes.c_int64)
+    rc = load().dtwj_pair_dtw(_dptr(a), a.size, m, w, pi.ctypes.data_as(P64),
+                              pj.ctypes.data_as(P64), pi.size, 1 if precise else 0, _dptr(out))
+    if rc != OK:
+        raise DtwjError(rc, "dtwj_pair_dtw")
+    return out
+
+
+def dtw_motif_discovery(ts, subseqlen: int, maxwarp: int, output_time_file_path: str,
+                        flags: int = 0, quiet: bool = False) -> JoinResult:
+    """Mirror of DTWMotifDiscoveryGUI (CPU_version1/DTWMotifDiscoveryGUI.cpp:12):
+    join, print the reference's result lines (1-based indices), append the
+    join time as "%lf\\n" to output_time_file_path."""
+    r = join(ts, subseqlen, maxwarp, flags)
+    if not quiet:
+        print("first min is %d sec min is %d" % (r.i + 1, r.j + 1))
+        print("total time is %fs   input of bsf:%5.3f  ,final distance :%f  "
+              % (r.seconds_join, r.seed_bsf, r.dist))
+    with open(output_time_file_path, "a") as f:
+        f.write("%f\n" % r.seconds_join)
+    return r

@@ -1,0 +1,132 @@
+// Internal header: device-side layout of one prepared series and the launch
+// entry points of every kernel of the join.  Host orchestration (join.cu)
+// only sees the launch functions declared at the bottom.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dtwj {
+
+// Relative slack on squared distances for every pruning and abandoning test.
+// FP32 distances and the FP64 diagonal recurrences carry rounding error far
+// below this; the slack keeps every pair whose true distance can still be the
+// minimum, and the final candidates are re-verified in FP64.
+constexpr float kSlack = 1.0f / 512.0f;
+// Endpoint bound width (the reference's BIAS, CPU_version1/diag_mask_global.cpp:8).
+constexpr int kBias = 3;
+// Seeds taken from the ED matrix profile (CPU_version1/new_dtw_motifGUI.cpp:53).
+constexpr int kSeeds = 100;
+// Sentinels padding the z-normalised sequences: finite so that no
+// inf - inf appears, far enough apart that any cell touching them is
+// effectively infinite.
+constexpr float kPadQ = 1e18f;
+constexpr float kPadT = -1e18f;
+constexpr double kPadQd = 1e150;
+constexpr double kPadTd = -1e150;
+
+// Lag-block x row-block of the diagonal sweep: pairs (i, i + L) for
+// L in [L0, L0 + kTileLags) and i in [i0, i0 + rows).
+struct Tile {
+  int32_t L0;
+  int32_t i0;
+  int32_t rows;
+  int32_t order;  // position in the queue order (learned or plain)
+};
+constexpr int kTileLags = 128;
+
+// Counters, all uint64 on the device.
+enum Counter {
+  kPairs = 0,
+  kPrunedFast,
+  kPrunedKim,
+  kPrunedMasked,
+  kPrunedKeogh,
+  kDtwCalls,
+  kDtwAbandoned,
+  kDtwCells,
+  kCandidates,
+  kNumCounters
+};
+
+struct Candidate {
+  int32_t i, j;
+  float d2;
+  int32_t pad;
+};
+
+// All device arrays of one prepared series.
+struct DevSeries {
+  const double* a;  // n, the series
+  int64_t n;
+  int64_t s;        // n - m + 1
+  int m, w;
+  double* mu;       // s, window mean
+  double* sig;      // s, window population std (1 for flat windows)
+  double* isg;      // s, 1/sig (0 for flat windows)
+  uint8_t* flat;    // s
+  double* U;        // n, upper envelope of the raw series, radius w
+  double* L;        // n, lower envelope
+  double* E;        // n, U + L
+  double* nu;       // s, mean of (U + L) over the window
+  double* dfa;      // s, (a[i+m] - a[i]) / 2
+  double* dga;      // s, (a[i+m] - mu[i+1]) + (a[i] - mu[i])
+  double* dfE;      // s, same for E = U + L
+  double* dgE;      // s
+  double* A;        // s, 4m + 2N - DUL2   (fast bound row constant)
+  double* DUL;      // s, ||nU - nL||
+  double* qsig;     // s, sig / 4 (1e300-guarded for flat windows)
+  float* mask;      // n, 0/1 mask of the masked bound
+  float* MN;        // s, sum_T M (nU^2 + nL^2)
+  float* MDUL2;     // s, sum_m M (nU - nL)^2
+  float* MDUL;      // s
+  int* status;      // device status word (0 ok, else error bits)
+};
+
+// Global search state of one join.
+struct DevSearch {
+  unsigned int* bsf2;           // float bits of the best squared DTW so far
+  unsigned long long* counters; // kNumCounters
+  Candidate* cand;              // candidate list
+  unsigned int* cand_count;
+  unsigned int cand_cap;
+  int2* queue;                  // survivor pairs of the current chunk
+  unsigned int* queue_count;
+  unsigned int* queue_next;
+  unsigned int queue_cap;
+};
+
+struct BandShape {
+  int C;  // cells (diagonals) per lane
+  int G;  // lanes per pair
+};
+// Picks lanes-per-pair G in {4, 8, 16, 32} and cells-per-lane C in [2, 16]
+// covering 2w+1 diagonals with the least waste.  Returns false if w > 255.
+bool choose_band(int w, BandShape* out);
+
+// ---- launches (all on `stream`) ----
+void launch_check_finite(const double* a, int64_t n, int* status, cudaStream_t st);
+void launch_prep(const DevSeries& S, cudaStream_t st);
+void launch_rowterms(const DevSeries& S, bool masked, cudaStream_t st);
+// Largest CDF length the mask can need: max |z| <= sqrt(m - 1).
+int mask_table_max(int m);
+void launch_mask(const DevSeries& S, unsigned int* counts, int lt_max, double* diff,
+                 double* mean_acc, float* zmax, cudaStream_t st);
+void launch_mp(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long long* keys,
+               bool lower, cudaStream_t st);
+void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
+                        const unsigned long long* lo, double* mp, int64_t* mpi,
+                        cudaStream_t st);
+void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
+                        unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st);
+// enumerate_all: no pruning, every pair goes to the queue (bounds disabled)
+void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
+               int tile_end, bool enumerate_all, cudaStream_t st);
+void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
+                  const unsigned int* npairs, bool masked, bool bounds, BandShape band,
+                  int num_sms, cudaStream_t st);
+void launch_verify(const DevSeries& S, const DevSearch& Q, BandShape band, double* out_d2,
+                   double* best_d2, int* best_idx, cudaStream_t st);
+void launch_pair_dtw(const DevSeries& S, const int2* pairs, int count, bool precise,
+                     BandShape band, double* out_d2, cudaStream_t st);
+
+}  // namespace dtwj

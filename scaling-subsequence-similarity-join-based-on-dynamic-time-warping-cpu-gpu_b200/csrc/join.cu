@@ -1,0 +1,556 @@
+// Host orchestration of the join and the C ABI (include/dtwj.h).
+//
+// The reference's driver (GPU_version1/src/new_dtw_motifGUI_malloc.cu:30-816)
+// prepares everything on the host, allocates one device buffer per
+// subsequence and then loops over diagonal blocks with five launches and
+// three host synchronisations per block.  Here every phase runs on one
+// stream with device-resident state:
+//   prep      statistics, envelopes, mask, row constants        (prep.cu)
+//   profile   ED matrix profile, row minima                      (mp.cu)
+//   seeds     kSeeds smallest profile entries -> exact DTW        (mp.cu, pairs.cu)
+//   sweep     per chunk of tiles: diagonal bound -> survivor
+//             queue -> endpoint / masked / LB_Keogh / DTW         (lb.cu, pairs.cu)
+//   verify    FP64 DTW of every candidate near the final best     (pairs.cu)
+// with a single host synchronisation at the end.
+#include "../../include/dtwj.h"
+#include "dtwj_dev.cuh"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace dtwj;
+
+namespace {
+
+constexpr int kTileRows = 4096;
+constexpr unsigned int kCandCap = 1u << 20;
+constexpr unsigned int kQueueCapMax = 1u << 27;
+
+struct Buf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct Timer {
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  double seconds() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+
+}  // namespace
+
+struct dtwj_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  std::vector<Buf> bufs;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<Tile> tiles_host;
+  int64_t tiles_n = -1, tiles_m = -1;
+};
+
+namespace {
+
+enum BufId {
+  B_A = 0, B_MU, B_SIG, B_ISG, B_FLAT, B_U, B_L, B_E, B_NU, B_DFA, B_DGA, B_DFE, B_DGE,
+  B_AC, B_DUL, B_QSIG, B_MASK, B_MN, B_MDUL2, B_MDUL, B_STATUS,
+  B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_KEYS_LO, B_TILES, B_QUEUE, B_QCOUNT,
+  B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
+  B_MP, B_MPI,
+  B_COUNT_
+};
+
+int ensure(dtwj_ctx* c, int id, size_t bytes, void** out) {
+  if (c->bufs.size() < (size_t)B_COUNT_) c->bufs.resize(B_COUNT_);
+  Buf& b = c->bufs[id];
+  if (b.cap < bytes) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t want = bytes < 256 ? 256 : bytes;
+    if (cudaMalloc(&b.p, want) != cudaSuccess) {
+      cudaGetLastError();
+      return DTWJ_ERR_OOM;
+    }
+    b.cap = want;
+  }
+  *out = b.p;
+  return DTWJ_OK;
+}
+
+#define ENSURE(id, bytes, ptr)                                       \
+  do {                                                               \
+    void* _p = nullptr;                                              \
+    int _rc = ensure(ctx, id, (size_t)(bytes), &_p);                 \
+    if (_rc) return _rc;                                             \
+    ptr = reinterpret_cast<decltype(ptr)>(_p);                       \
+  } while (0)
+
+#define CUDA_OK(expr)                                                 \
+  do {                                                                \
+    cudaError_t _e = (expr);                                          \
+    if (_e != cudaSuccess) {                                          \
+      if (getenv("DTWJ_DEBUG"))                                       \
+        fprintf(stderr, "dtwj: %s failed: %s\n", #expr, cudaGetErrorString(_e)); \
+      return DTWJ_ERR_CUDA;                                           \
+    }                                                                 \
+  } while (0)
+
+int check_args(const void* x, int64_t n, int32_t m, int32_t w) {
+  if (!x || m < 8 || w < 0) return DTWJ_ERR_ARG;
+  if (n < 2 * (int64_t)m + 1 || n > (int64_t)INT32_MAX - 4) return DTWJ_ERR_ARG;
+  return DTWJ_OK;
+}
+
+void build_tiles(dtwj_ctx* ctx, int64_t n, int m) {
+  if (ctx->tiles_n == n && ctx->tiles_m == m) return;
+  const int64_t s = n - m + 1;
+  ctx->tiles_host.clear();
+  int32_t order = 0;
+  for (int64_t L0 = m; L0 <= s - 1; L0 += kTileLags) {
+    const int64_t rows_total = s - L0;
+    for (int64_t i0 = 0; i0 < rows_total; i0 += kTileRows) {
+      Tile t;
+      t.L0 = (int32_t)L0;
+      t.i0 = (int32_t)i0;
+      t.rows = (int32_t)(rows_total - i0 < kTileRows ? rows_total - i0 : kTileRows);
+      t.order = order++;
+      ctx->tiles_host.push_back(t);
+    }
+  }
+  ctx->tiles_n = n;
+  ctx->tiles_m = m;
+}
+
+// Allocates and prepares every per-series array; returns the DevSeries.
+int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool masked,
+            DevSeries* out) {
+  const int64_t s = n - m + 1;
+  DevSeries S;
+  memset(&S, 0, sizeof S);
+  S.a = x_dev;
+  S.n = n;
+  S.s = s;
+  S.m = m;
+  S.w = w;
+  ENSURE(B_MU, s * 8, S.mu);
+  ENSURE(B_SIG, s * 8, S.sig);
+  ENSURE(B_ISG, s * 8, S.isg);
+  ENSURE(B_FLAT, s, S.flat);
+  ENSURE(B_U, n * 8, S.U);
+  ENSURE(B_L, n * 8, S.L);
+  ENSURE(B_E, n * 8, S.E);
+  ENSURE(B_NU, s * 8, S.nu);
+  ENSURE(B_DFA, s * 8, S.dfa);
+  ENSURE(B_DGA, s * 8, S.dga);
+  ENSURE(B_DFE, s * 8, S.dfE);
+  ENSURE(B_DGE, s * 8, S.dgE);
+  ENSURE(B_AC, s * 8, S.A);
+  ENSURE(B_DUL, s * 8, S.DUL);
+  ENSURE(B_QSIG, s * 8, S.qsig);
+  ENSURE(B_MASK, n * 4, S.mask);
+  ENSURE(B_MN, s * 4, S.MN);
+  ENSURE(B_MDUL2, s * 4, S.MDUL2);
+  ENSURE(B_MDUL, s * 4, S.MDUL);
+  ENSURE(B_STATUS, 4, S.status);
+  cudaStream_t st = ctx->stream;
+  CUDA_OK(cudaMemsetAsync(S.status, 0, 4, st));
+  launch_check_finite(S.a, n, S.status, st);
+  int status = 0;
+  CUDA_OK(cudaMemcpyAsync(&status, S.status, 4, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  if (status & 1) return DTWJ_ERR_NAN;
+  launch_prep(S, st);
+  if (masked) {
+    const int lt_max = mask_table_max(m);
+    unsigned int* counts;
+    double* diff;
+    double* mean;
+    float* zmax;
+    ENSURE(B_COUNTS, (size_t)m * lt_max * 4, counts);
+    ENSURE(B_DIFF, n * 8, diff);
+    ENSURE(B_MEAN, 8, mean);
+    ENSURE(B_ZMAX, 4, zmax);
+    launch_mask(S, counts, lt_max, diff, mean, zmax, st);
+  } else {
+    CUDA_OK(cudaMemsetAsync(S.mask, 0, n * 4, st));
+  }
+  launch_rowterms(S, masked, st);
+  CUDA_OK(cudaGetLastError());
+  *out = S;
+  return DTWJ_OK;
+}
+
+int effective_band(int m, int w) { return w > m - 1 ? m - 1 : w; }
+
+int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_t w_in,
+                uint32_t flags, dtwj_result* out, double t_upload) {
+  Timer wall;
+  const int w = effective_band(m, w_in);
+  BandShape band;
+  if (!choose_band(w, &band)) return DTWJ_ERR_BAND;
+  if (flags & DTWJ_F_LEARNED) return DTWJ_ERR_NOMODEL;
+  const bool masked = !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
+  const bool verbose = flags & DTWJ_F_VERBOSE;
+  cudaStream_t st = ctx->stream;
+  CUDA_OK(cudaEventRecord(ctx->ev0, st));
+
+  DevSeries S;
+  int rc = prepare(ctx, x_dev, n, m, w, masked, &S);
+  if (rc) return rc;
+  const int64_t s = S.s;
+
+  build_tiles(ctx, n, m);
+  const int ntiles = (int)ctx->tiles_host.size();
+  Tile* tiles;
+  ENSURE(B_TILES, (size_t)ntiles * sizeof(Tile), tiles);
+  CUDA_OK(cudaMemcpyAsync(tiles, ctx->tiles_host.data(), (size_t)ntiles * sizeof(Tile),
+                          cudaMemcpyHostToDevice, st));
+
+  // search state
+  DevSearch Q;
+  memset(&Q, 0, sizeof Q);
+  const double total_pairs = 0.5 * (double)(s - m) * (double)(s - m + 1);
+  unsigned int qcap = kQueueCapMax;
+  if (total_pairs < (double)qcap) qcap = (unsigned int)total_pairs + 1024;
+  const int tiles_per_chunk_max = (int)(qcap / ((unsigned)kTileLags * kTileRows));
+  ENSURE(B_QUEUE, (size_t)qcap * sizeof(int2), Q.queue);
+  unsigned int* qc;
+  ENSURE(B_QCOUNT, 16, qc);
+  Q.queue_count = qc;
+  Q.queue_next = qc + 1;
+  Q.queue_cap = qcap;
+  ENSURE(B_BSF2, 4, Q.bsf2);
+  ENSURE(B_COUNTERS, kNumCounters * 8, Q.counters);
+  ENSURE(B_CAND, (size_t)kCandCap * sizeof(Candidate), Q.cand);
+  ENSURE(B_CCOUNT, 4, Q.cand_count);
+  Q.cand_cap = kCandCap;
+  CUDA_OK(cudaMemsetAsync(Q.counters, 0, kNumCounters * 8, st));
+  CUDA_OK(cudaMemsetAsync(Q.cand_count, 0, 4, st));
+  const unsigned int inf_bits = 0x7f800000u;
+  CUDA_OK(cudaMemcpyAsync(Q.bsf2, &inf_bits, 4, cudaMemcpyHostToDevice, st));
+
+  // ---- ED profile seeds ----
+  float seed_bsf2 = INFINITY;
+  if (!(flags & DTWJ_F_NO_SEED)) {
+    unsigned long long* keys;
+    ENSURE(B_KEYS_UP, s * 8, keys);
+    launch_mp(S, tiles, ntiles, keys, false, st);
+    int2* seeds;
+    unsigned int* nseeds;
+    ENSURE(B_SEEDS, kSeeds * sizeof(int2), seeds);
+    ENSURE(B_NSEEDS, 16, nseeds);
+    CUDA_OK(cudaMemsetAsync(nseeds, 0, 16, st));
+    launch_seed_select(S, keys, seeds, nseeds, Q.bsf2, st);
+    CUDA_OK(cudaMemsetAsync(nseeds + 1, 0, 4, st));
+    DevSearch Qs = Q;
+    Qs.queue_next = nseeds + 1;
+    launch_pairs(S, Qs, seeds, nseeds, masked, false, band, ctx->num_sms, st);
+    unsigned int b2 = 0;
+    CUDA_OK(cudaMemcpyAsync(&b2, Q.bsf2, 4, cudaMemcpyDeviceToHost, st));
+    if (verbose) {
+      CUDA_OK(cudaStreamSynchronize(st));
+      memcpy(&seed_bsf2, &b2, 4);
+      fprintf(stderr, "dtwj: seeds done, bsf %.6f, %.3fs\n", std::sqrt(seed_bsf2), wall.seconds());
+    } else {
+      CUDA_OK(cudaStreamSynchronize(st));
+      memcpy(&seed_bsf2, &b2, 4);
+    }
+  }
+
+  // ---- diagonal sweep in chunks ----
+  const bool enumerate_all = flags & DTWJ_F_NO_DIAG;
+  int chunk = tiles_per_chunk_max > 0 ? tiles_per_chunk_max : 1;
+  for (int t0 = 0; t0 < ntiles; t0 += chunk) {
+    const int t1 = t0 + chunk < ntiles ? t0 + chunk : ntiles;
+    CUDA_OK(cudaMemsetAsync(qc, 0, 8, st));
+    launch_lb(S, Q, tiles, t0, t1, enumerate_all, st);
+    launch_pairs(S, Q, Q.queue, Q.queue_count, masked, !enumerate_all, band, ctx->num_sms, st);
+  }
+  CUDA_OK(cudaGetLastError());
+
+  // ---- FP64 verification of the candidates ----
+  double* vd2;
+  ENSURE(B_VERIFY, (size_t)kCandCap * 8, vd2);
+  double* best;
+  ENSURE(B_BEST, 16, best);
+  int* best_idx = reinterpret_cast<int*>(best + 1);
+  launch_verify(S, Q, band, vd2, best, best_idx, st);
+  CUDA_OK(cudaEventRecord(ctx->ev1, st));
+
+  double best_h[2];
+  unsigned long long cnt_h[kNumCounters];
+  unsigned int cand_h = 0, bsf_h = 0;
+  int status_h = 0;
+  CUDA_OK(cudaMemcpyAsync(best_h, best, 16, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(cnt_h, Q.counters, sizeof cnt_h, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(&cand_h, Q.cand_count, 4, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(&bsf_h, Q.bsf2, 4, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(&status_h, S.status, 4, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaStreamSynchronize(st));
+  if (status_h & 2) return DTWJ_ERR_OVERFLOW;
+  if (cand_h > kCandCap) return DTWJ_ERR_OVERFLOW;
+  int bidx;
+  memcpy(&bidx, &best_h[1], 4);
+  Candidate bc;
+  memset(&bc, 0, sizeof bc);
+  if (bidx >= 0) {
+    CUDA_OK(cudaMemcpy(&bc, Q.cand + bidx, sizeof bc, cudaMemcpyDeviceToHost));
+  }
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+
+  memset(out, 0, sizeof *out);
+  out->n = n;
+  out->m = m;
+  out->w = w_in;
+  if (bidx >= 0) {
+    out->i = bc.i;
+    out->j = bc.j;
+    out->dist = std::sqrt(best_h[0]);
+    out->dist_fp32 = std::sqrt((double)bc.d2);
+  } else {
+    out->i = out->j = -1;
+    out->dist = out->dist_fp32 = INFINITY;
+  }
+  out->seed_bsf = std::sqrt((double)seed_bsf2);
+  out->pairs = cnt_h[kPairs];
+  out->pruned_fast = cnt_h[kPrunedFast];
+  out->pruned_kim = cnt_h[kPrunedKim];
+  out->pruned_masked = cnt_h[kPrunedMasked];
+  out->pruned_keogh = cnt_h[kPrunedKeogh];
+  out->dtw_calls = cnt_h[kDtwCalls];
+  out->dtw_abandoned = cnt_h[kDtwAbandoned];
+  out->dtw_cells = cnt_h[kDtwCells];
+  out->candidates = cand_h;
+  out->seconds_join = ms / 1000.0;
+  out->seconds_total = wall.seconds() + t_upload;
+  (void)bsf_h;
+  if (verbose)
+    fprintf(stderr, "dtwj: join (%lld, %lld) %.6f, %.3fs device\n", (long long)out->i,
+            (long long)out->j, out->dist, out->seconds_join);
+  return DTWJ_OK;
+}
+
+int upload(dtwj_ctx* ctx, const double* x, int64_t n, double** dev) {
+  ENSURE(B_A, n * 8, *dev);
+  CUDA_OK(cudaMemcpyAsync(*dev, x, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  return DTWJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dtwj_device_count(void) {
+  int c = 0;
+  if (cudaGetDeviceCount(&c) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return c;
+}
+
+int dtwj_ctx_create(int device, dtwj_ctx** out) {
+  if (!out) return DTWJ_ERR_ARG;
+  *out = nullptr;
+  if (dtwj_device_count() <= device || device < 0) return DTWJ_ERR_NODEVICE;
+  dtwj_ctx* c = new (std::nothrow) dtwj_ctx();
+  if (!c) return DTWJ_ERR_OOM;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete c;
+    return DTWJ_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    delete c;
+    return DTWJ_ERR_CUDA;
+  }
+  c->bufs.resize(B_COUNT_);
+  *out = c;
+  return DTWJ_OK;
+}
+
+void dtwj_ctx_destroy(dtwj_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& b : c->bufs)
+    if (b.p) cudaFree(b.p);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int dtwj_ctx_join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_t w,
+                         uint32_t flags, dtwj_result* out) {
+  if (!ctx || !out) return DTWJ_ERR_ARG;
+  int rc = check_args(x_dev, n, m, w);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  return join_device(ctx, x_dev, n, m, w, flags, out, 0.0);
+}
+
+int dtwj_ctx_join(dtwj_ctx* ctx, const double* x, int64_t n, int32_t m, int32_t w,
+                  uint32_t flags, dtwj_result* out) {
+  if (!ctx || !out) return DTWJ_ERR_ARG;
+  int rc = check_args(x, n, m, w);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  Timer t;
+  double* dev = nullptr;
+  rc = upload(ctx, x, n, &dev);
+  if (rc) return rc;
+  rc = join_device(ctx, dev, n, m, w, flags, out, 0.0);
+  if (rc == DTWJ_OK) out->seconds_total = t.seconds();
+  return rc;
+}
+
+int dtwj_join(const double* x, int64_t n, int32_t m, int32_t w, uint32_t flags,
+              dtwj_result* out) {
+  if (!out) return DTWJ_ERR_ARG;
+  int rc = check_args(x, n, m, w);
+  if (rc) return rc;
+  dtwj_ctx* ctx = nullptr;
+  rc = dtwj_ctx_create(0, &ctx);
+  if (rc) return rc;
+  rc = dtwj_ctx_join(ctx, x, n, m, w, flags, out);
+  dtwj_ctx_destroy(ctx);
+  return rc;
+}
+
+int dtwj_join_batch(const double* const* xs, const int64_t* ns, const int32_t* ms,
+                    const int32_t* ws, int32_t count, uint32_t flags, dtwj_result* outs) {
+  if (!xs || !ns || !ms || !ws || !outs || count < 0) return DTWJ_ERR_ARG;
+  dtwj_ctx* ctx = nullptr;
+  int rc = dtwj_ctx_create(0, &ctx);
+  if (rc) return rc;
+  for (int32_t k = 0; k < count && rc == DTWJ_OK; ++k)
+    rc = dtwj_ctx_join(ctx, xs[k], ns[k], ms[k], ws[k], flags, &outs[k]);
+  dtwj_ctx_destroy(ctx);
+  return rc;
+}
+
+int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64_t* mpi) {
+  if (!mp || !mpi) return DTWJ_ERR_ARG;
+  int rc = check_args(x, n, m, 0);
+  if (rc) return rc;
+  dtwj_ctx* ctx = nullptr;
+  rc = dtwj_ctx_create(0, &ctx);
+  if (rc) return rc;
+  do {
+    double* dev = nullptr;
+    if ((rc = upload(ctx, x, n, &dev))) break;
+    DevSeries S;
+    if ((rc = prepare(ctx, dev, n, m, 0, false, &S))) break;
+    build_tiles(ctx, n, m);
+    const int ntiles = (int)ctx->tiles_host.size();
+    Tile* tiles;
+    void* p;
+    if ((rc = ensure(ctx, B_TILES, (size_t)ntiles * sizeof(Tile), &p))) break;
+    tiles = (Tile*)p;
+    cudaMemcpyAsync(tiles, ctx->tiles_host.data(), (size_t)ntiles * sizeof(Tile),
+                    cudaMemcpyHostToDevice, ctx->stream);
+    const int64_t s = n - m + 1;
+    if ((rc = ensure(ctx, B_KEYS_UP, s * 8, &p))) break;
+    unsigned long long* up = (unsigned long long*)p;
+    if ((rc = ensure(ctx, B_KEYS_LO, s * 8, &p))) break;
+    unsigned long long* lo = (unsigned long long*)p;
+    launch_mp(S, tiles, ntiles, up, false, ctx->stream);
+    launch_mp(S, tiles, ntiles, lo, true, ctx->stream);
+    if ((rc = ensure(ctx, B_MP, s * 8, &p))) break;
+    double* dmp = (double*)p;
+    if ((rc = ensure(ctx, B_MPI, s * 8, &p))) break;
+    int64_t* dmpi = (int64_t*)p;
+    launch_mp_finalize(S, up, lo, dmp, dmpi, ctx->stream);
+    if (cudaMemcpyAsync(mp, dmp, s * 8, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaMemcpyAsync(mpi, dmpi, s * 8, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      rc = DTWJ_ERR_CUDA;
+      break;
+    }
+  } while (0);
+  dtwj_ctx_destroy(ctx);
+  return rc;
+}
+
+int dtwj_pair_dtw(const double* x, int64_t n, int32_t m, int32_t w, const int64_t* pi,
+                  const int64_t* pj, int64_t count, int32_t precise, double* dist) {
+  if (!pi || !pj || !dist || count < 0) return DTWJ_ERR_ARG;
+  int rc = check_args(x, n, m, w);
+  if (rc) return rc;
+  const int64_t s = n - m + 1;
+  std::vector<int2> pairs((size_t)count);
+  for (int64_t k = 0; k < count; ++k) {
+    if (pi[k] < 0 || pj[k] < 0 || pi[k] >= s || pj[k] >= s) return DTWJ_ERR_ARG;
+    pairs[k] = make_int2((int)pi[k], (int)pj[k]);
+  }
+  if (count == 0) return DTWJ_OK;
+  const int we = effective_band(m, w);
+  BandShape band;
+  if (!choose_band(we, &band)) return DTWJ_ERR_BAND;
+  dtwj_ctx* ctx = nullptr;
+  rc = dtwj_ctx_create(0, &ctx);
+  if (rc) return rc;
+  do {
+    double* dev = nullptr;
+    if ((rc = upload(ctx, x, n, &dev))) break;
+    DevSeries S;
+    if ((rc = prepare(ctx, dev, n, m, we, false, &S))) break;
+    void* p;
+    if ((rc = ensure(ctx, B_PAIRS, (size_t)count * sizeof(int2), &p))) break;
+    int2* dp = (int2*)p;
+    if ((rc = ensure(ctx, B_OUT, (size_t)count * 8, &p))) break;
+    double* dout = (double*)p;
+    cudaMemcpyAsync(dp, pairs.data(), (size_t)count * sizeof(int2), cudaMemcpyHostToDevice,
+                    ctx->stream);
+    launch_pair_dtw(S, dp, (int)count, precise != 0, band, dout, ctx->stream);
+    if (cudaMemcpyAsync(dist, dout, (size_t)count * 8, cudaMemcpyDeviceToHost, ctx->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      rc = DTWJ_ERR_CUDA;
+      break;
+    }
+    for (int64_t k = 0; k < count; ++k) dist[k] = std::sqrt(dist[k]);
+  } while (0);
+  dtwj_ctx_destroy(ctx);
+  return rc;
+}
+
+int32_t dtwj_band(int32_t m, double ratio, int32_t rounding) {
+  double v = ratio * (double)m;
+  int32_t w;
+  if (rounding == 1) w = (int32_t)std::floor(v + 0.5);
+  else w = (int32_t)std::ceil(v - 1e-9);
+  return w < 1 ? 1 : w;
+}
+
+const char* dtwj_strerror(int code) {
+  switch (code) {
+    case DTWJ_OK: return "ok";
+    case DTWJ_ERR_ARG: return "invalid argument";
+    case DTWJ_ERR_NAN: return "input contains NaN or infinity";
+    case DTWJ_ERR_CUDA: return "CUDA error";
+    case DTWJ_ERR_OOM: return "device out of memory";
+    case DTWJ_ERR_BAND: return "band too wide (w must be <= 255)";
+    case DTWJ_ERR_OVERFLOW: return "candidate or survivor list overflow";
+    case DTWJ_ERR_TIMEOUT: return "device-side wait ran out";
+    case DTWJ_ERR_NODEVICE: return "no CUDA device";
+    case DTWJ_ERR_IO: return "file could not be read or written";
+    case DTWJ_ERR_NOMODEL: return "learned ordering requested but no model is loaded";
+    default: return "unknown error";
+  }
+}
+
+}  // extern "C"

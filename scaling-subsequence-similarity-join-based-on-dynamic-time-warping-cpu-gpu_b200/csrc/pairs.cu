@@ -1,0 +1,696 @@
+// Per-pair stages: endpoint bound, masked diagonal bound, LB_Keogh in both
+// directions with its cumulative bound, and the banded DTW itself.
+//
+// Reference counterparts:
+//   endpoint bound  LB_KIM / the tail of diag_mask_global
+//                   CPU_version1/lb_kim.cpp:10-73, GPU_version1/lib/diag_mask_global.cu:165-228
+//   masked bound    diag_mask_global  CPU_version1/diag_mask_global.cpp:11-226
+//   LB_Keogh        LB_KK             CPU_version1/lb_keogh.cpp:9-72,
+//                   lb_keogh_stride_with_nomalise  GPU_version1/src/LB_keogh_warp.cu:74-96
+//   DTW             MON_dtw           CPU_version1/MON_DTW.cpp:20-108,
+//                   DTW_stairs_*      GPU_version1/src/DTW_stairs*.cu
+//   bsf update      atomicMinFloat + syn_bsfs  GPU_version1/lib/GLOBAL_DIAG.cu:18-27
+//
+// Band layout (the register "stairs" of the reference, with the band width a
+// runtime template choice instead of the REGISTER_NUM recompile): a group of
+// G lanes computes one pair; lane g owns the C consecutive diagonals
+// d = -w + gC .. -w + gC + C - 1 (cell (r, r + d)).  Lane g handles row
+// r = tau - g at step tau: cell (r, d) needs (r, d-1) from the left lane's
+// previous step (shfl_up of its last cell) and (r-1, d+1) from the right
+// lane's first cell of this step (shfl_down right after it is computed), so
+// every lane computes a full row of its C cells per step with two shuffles.
+// q and t are z-normalised in shared memory with finite sentinels outside
+// [0, m) so out-of-range cells are effectively infinite without branches.
+#include "dtwj_dev.cuh"
+
+#include <cfloat>
+#include <climits>
+
+namespace dtwj {
+namespace {
+
+template <typename T> struct Pad;
+template <> struct Pad<float> {
+  static __device__ __forceinline__ float q() { return kPadQ; }
+  static __device__ __forceinline__ float t() { return kPadT; }
+  static __device__ __forceinline__ float inf() { return __int_as_float(0x7f800000); }
+};
+template <> struct Pad<double> {
+  static __device__ __forceinline__ double q() { return kPadQd; }
+  static __device__ __forceinline__ double t() { return kPadTd; }
+  static __device__ __forceinline__ double inf() { return __longlong_as_double(0x7ff0000000000000LL); }
+};
+
+__device__ __forceinline__ float fmin_(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double fmin_(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float fmax_(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fmax_(double a, double b) { return fmax(a, b); }
+
+template <int G>
+__device__ __forceinline__ unsigned int group_mask() {
+  if (G == 32) return 0xffffffffu;
+  const unsigned int lane = threadIdx.x & 31;
+  return ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
+}
+
+template <int G, typename V>
+__device__ __forceinline__ V group_sum(V v, unsigned int gm) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gm, v, o, G);
+  return v;
+}
+
+// Shared-memory footprint of one group (in elements of T).
+struct GroupLayout {
+  int pq, pt;     // padding of q and t on each side
+  int nc;         // cumulative-bound chunks
+  int e2;         // edge prefix/suffix length
+  int q_off, t_off, cb_off, edge_off, total;
+};
+
+__host__ __device__ inline GroupLayout group_layout(int m, int w, int C, int G, bool bounds) {
+  GroupLayout l;
+  l.pq = G + 1;
+  l.pt = G * C + G + 2;  // t is read at offsets [-(G + w), m + G + GC)
+  l.nc = (m + 7) / 8;
+  l.e2 = m < 2 * w ? m : 2 * w;
+  if (l.e2 < 1) l.e2 = 1;
+  l.q_off = l.pq;
+  l.t_off = l.pq + m + l.pq + l.pt;
+  l.cb_off = l.t_off + m + l.pt;
+  l.edge_off = l.cb_off + l.nc + 2;
+  l.total = l.edge_off + (bounds ? 8 * l.e2 : 0);
+  l.total = (l.total + 3) & ~3;
+  return l;
+}
+
+// Banded DTW of q (rows) against t (columns), squared cost.  With ABANDON the
+// group stops as soon as every lane's latest row, plus the cumulative bound
+// of the rows and columns still ahead, exceeds the threshold; it then returns
+// +inf and reports the cells it swept.
+template <typename T, int C, int G, bool ABANDON>
+__device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, int w,
+                      const float* __restrict__ cbc, int nc, float thr,
+                      const unsigned int* bsf2, unsigned int gm, int g,
+                      unsigned long long* cells, bool* abandoned) {
+  const T INF = Pad<T>::inf();
+  const int d_lo = -w + g * C;
+  T pen[C], prev[C], cur[C], tw[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    pen[c] = (d_lo + c <= w) ? T(0) : INF;
+    prev[c] = (d_lo + c == 0) ? T(0) : INF;
+    tw[c] = t[-g + d_lo + c];
+  }
+  const int g0 = w / C, c0 = w % C;
+  const int tau_end = m - 1 + g0;
+  T last = INF;
+  T result = INF;
+  *abandoned = false;
+  for (int tau = 0; tau <= tau_end; ++tau) {
+    const int r = tau - g;
+    T left = __shfl_up_sync(gm, last, 1, G);
+    if (g == 0) left = INF;
+    const T qr = q[r];
+    {
+      const T d = qr - tw[0];
+      T v = fmin_(fmin_(prev[1 < C ? 1 : 0], prev[0]), left);
+      v = fmax_(fma(d, d, v), pen[0]);
+      cur[0] = v;
+    }
+    T right = __shfl_down_sync(gm, cur[0], 1, G);
+    if (g == G - 1) right = INF;
+#pragma unroll
+    for (int c = 1; c < C; ++c) {
+      const T up = (c + 1 < C) ? prev[c + 1 < C ? c + 1 : 0] : right;
+      const T d = qr - tw[c];
+      T v = fmin_(fmin_(up, prev[c]), cur[c - 1]);
+      v = fmax_(fma(d, d, v), pen[c]);
+      cur[c] = v;
+    }
+    last = cur[C - 1];
+    if (tau == tau_end && g == g0) {
+#pragma unroll
+      for (int c = 0; c < C; ++c)
+        if (c == c0) result = cur[c];
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) prev[c] = cur[c];
+#pragma unroll
+    for (int c = 0; c < C - 1; ++c) tw[c] = tw[c + 1];
+    tw[C - 1] = t[r + d_lo + C];
+    if (ABANDON && (tau & 15) == 15 && tau < tau_end) {
+      T fm = cur[0];
+#pragma unroll
+      for (int c = 1; c < C; ++c) fm = fmin_(fm, cur[c]);
+      int idx = r + w + 1;
+      idx = idx < 0 ? 0 : (idx + 7) >> 3;
+      const float cbv = cbc[idx < nc ? idx : nc];
+      const float fresh = __uint_as_float(*(volatile const unsigned int*)bsf2) * (1.0f + kSlack);
+      thr = fminf(thr, fresh);
+      const bool over = (float)fm + cbv > thr;
+      const unsigned int vote = __ballot_sync(gm, over);
+      if ((vote & gm) == gm) {
+        // cells swept so far: rows [0, rows_done) of each owned diagonal
+        const int rows_done = r + 1 < 0 ? 0 : (r + 1 > m ? m : r + 1);
+        unsigned long long cnt = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const int d = d_lo + c;
+          if (d > w) continue;
+          const int lo = d < 0 ? -d : 0;
+          const int hi = rows_done < m - d ? rows_done : m - d;
+          if (hi > lo) cnt += (unsigned long long)(hi - lo);
+        }
+        *cells = group_sum<G>(cnt, gm);
+        *abandoned = true;
+        return INF;
+      }
+    }
+  }
+  result = __shfl_sync(gm, result, g0, G);
+  *cells = (unsigned long long)m * (2 * w + 1) - (unsigned long long)w * (w + 1);
+  return result;
+}
+
+// Endpoint bound: minimum cost of any warping path's cells in the first and
+// last three layers (LB_KIM, CPU_version1/lb_kim.cpp:10-73).  q = window i,
+// t = window j; the reference's fourth option adds the corner twice
+// (lb_kim.cpp:55,62), here it is added once so the bound stays admissible.
+__device__ void kim_bound(const float* q, const float* t, int m, float* left, float* right) {
+#define D2(x, y) (((x) - (y)) * ((x) - (y)))
+  const float o = D2(t[0], q[0]);
+  const float lw = fminf(D2(t[1], q[0]), D2(t[1], q[1]));
+  const float l1 = fminf(lw, D2(t[0], q[1]));
+  float d = fminf(D2(t[1], q[0]) + D2(t[2], q[0]), lw + D2(t[2], q[1]));
+  d = fminf(d, D2(q[1], t[1]) + D2(q[2], t[2]));
+  d = fminf(d, l1 + D2(q[2], t[1]));
+  d = fminf(d, D2(q[1], t[0]) + D2(q[2], t[0]));
+  *left = o + d;
+  const int e = m - 1;
+  const float o2 = D2(t[e], q[e]);
+  const float rw = fminf(D2(t[e - 1], q[e]), D2(t[e - 1], q[e - 1]));
+  const float r1 = fminf(rw, D2(t[e], q[e - 1]));
+  d = fminf(D2(t[e - 1], q[e]) + D2(t[e - 2], q[e]), rw + D2(t[e - 2], q[e - 1]));
+  d = fminf(d, D2(q[e - 1], t[e - 1]) + D2(q[e - 2], t[e - 2]));
+  d = fminf(d, r1 + D2(q[e - 2], t[e - 1]));
+  d = fminf(d, D2(q[e - 1], t[e]) + D2(q[e - 2], t[e]));
+  *right = o2 + d;
+#undef D2
+}
+
+// Envelope of z-normalised window `sub` (subs_U / subs_L of the reference) at
+// offset k: raw envelope in the interior, prefix / suffix extremes of the
+// window near its ends (the clipped window of lower_upper_lemire).
+struct EdgeEnv {
+  const float *pu, *pl, *su, *sl;  // prefix max/min [0, e2), suffix max/min [m-e2, m)
+  int e2;
+};
+
+__device__ __forceinline__ void envelope_at(const DevSeries& S, int64_t sub, double mu,
+                                            double isg, const EdgeEnv& E, int k, float* U,
+                                            float* L) {
+  const int m = S.m, w = S.w;
+  if (k < w) {
+    const int p = k + w < m - 1 ? k + w : m - 1;
+    *U = E.pu[p];
+    *L = E.pl[p];
+  } else if (k > m - 1 - w) {
+    const int p = (k - w > 0 ? k - w : 0) - (m - E.e2);
+    *U = E.su[p];
+    *L = E.sl[p];
+  } else {
+    *U = (float)((S.U[sub + k] - mu) * isg);
+    *L = (float)((S.L[sub + k] - mu) * isg);
+  }
+}
+
+__device__ __forceinline__ float keogh_term(float x, float U, float L) {
+  const float du = x - U, dl = x - L;
+  return x > U ? du * du : (x < L ? dl * dl : 0.0f);
+}
+
+// The pair consumer: every group takes pairs from the queue until it is
+// drained.  flags bit 0: run the bounds (otherwise DTW only, for seeds);
+// bit 1: run the masked bound.
+template <int C, int G>
+__global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const int2* pairs,
+                                                const unsigned int* npairs, int flags,
+                                                int group_floats) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float* sm = reinterpret_cast<float*>(smraw);
+  __shared__ unsigned long long cnt[kNumCounters];
+  const bool bounds = flags & 1, masked = flags & 2;
+  const int m = S.m, w = S.w;
+  const int gib = threadIdx.x / G, g = threadIdx.x % G;
+  const unsigned int gm = group_mask<G>();
+  const GroupLayout lay = group_layout(m, w, C, G, bounds);
+  float* base = sm + (size_t)gib * group_floats;
+  float* q = base + lay.q_off;
+  float* t = base + lay.t_off;
+  float* cbc = base + lay.cb_off;
+  float* edge = base + lay.edge_off;
+  for (int x = threadIdx.x; x < kNumCounters; x += blockDim.x) cnt[x] = 0;
+  // sentinels (written once; the interior is rewritten per pair)
+  for (int x = g; x < lay.pq; x += G) {
+    q[-1 - x] = kPadQ;
+    q[m + x] = kPadQ;
+  }
+  for (int x = g; x < lay.pt; x += G) {
+    t[-1 - x] = kPadT;
+    t[m + x] = kPadT;
+  }
+  __syncthreads();
+  const unsigned int total = *npairs;
+  for (;;) {
+    unsigned int idx = 0;
+    if (g == 0) idx = atomicAdd(Q.queue_next, 1u);
+    idx = __shfl_sync(gm, idx, 0, G);
+    if (idx >= total) break;
+    const int2 pr = pairs[idx];
+    const int64_t i = pr.x, j = pr.y;
+    const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
+    float thr = __uint_as_float(*(volatile unsigned int*)Q.bsf2) * (1.0f + kSlack);
+    for (int k = g; k < m; k += G) {
+      q[k] = (float)((S.a[i + k] - mi) * si);
+      t[k] = (float)((S.a[j + k] - mj) * sj);
+    }
+    for (int x = g; x <= lay.nc + 1; x += G) cbc[x] = 0.0f;
+    __syncwarp(gm);
+    if (bounds) {
+      // ---- endpoint bound ----
+      float kl = 0.0f, kr = 0.0f;
+      if (g == 0) kim_bound(q, t, m, &kl, &kr);
+      kl = __shfl_sync(gm, kl, 0, G);
+      kr = __shfl_sync(gm, kr, 0, G);
+      if (kl + kr > thr) {
+        if (g == 0) atomicAdd(&cnt[kPrunedKim], 1ull);
+        __syncwarp(gm);
+        continue;
+      }
+      // ---- masked diagonal bound (diag_mask_global) ----
+      if (masked) {
+        float s1 = 0, s2 = 0, r1 = 0, r2 = 0;
+        for (int k = kBias + g; k <= m - 1 - kBias; k += G) {
+          const float Mi = S.mask[i + k], Mj = S.mask[j + k];
+          const float ei = (float)((S.E[i + k] - 2.0 * mi) * si);
+          const float ej = (float)((S.E[j + k] - 2.0 * mj) * sj);
+          const float qj = t[k], qi = q[k];
+          s1 = fmaf(Mi * qj, qj, s1);
+          s2 = fmaf(Mi * qj, ei, s2);
+          r1 = fmaf(Mj * qi, qi, r1);
+          r2 = fmaf(Mj * qi, ej, r2);
+        }
+        s1 = group_sum<G>(s1, gm);
+        s2 = group_sum<G>(s2, gm);
+        r1 = group_sum<G>(r1, gm);
+        r2 = group_sum<G>(r2, gm);
+        const float df = 2.0f * s1 - 2.0f * s2 + S.MN[i];
+        const float dr = 2.0f * r1 - 2.0f * r2 + S.MN[j];
+        const float lf = df < S.MDUL2[i] ? 0.0f : 0.5f * (sqrtf(2.0f * df - S.MDUL2[i]) - S.MDUL[i]);
+        const float lr = dr < S.MDUL2[j] ? 0.0f : 0.5f * (sqrtf(2.0f * dr - S.MDUL2[j]) - S.MDUL[j]);
+        const float lbm = fmaxf(lf, lr);
+        if (lbm > 0.0f && lbm * lbm > thr) {
+          if (g == 0) atomicAdd(&cnt[kPrunedMasked], 1ull);
+          __syncwarp(gm);
+          continue;
+        }
+        if (kl + kr + lbm * lbm > thr) {
+          if (g == 0) atomicAdd(&cnt[kPrunedKim], 1ull);
+          __syncwarp(gm);
+          continue;
+        }
+      }
+      // ---- clipped envelopes near the window ends ----
+      {
+        const int e2 = lay.e2;
+        for (int sc = g; sc < 8; sc += G) {
+          const float* z = (sc >> 2) ? t : q;
+          float* out = edge + sc * e2;
+          const int kind = sc & 3;
+          if (kind < 2) {
+            float acc = z[0];
+            for (int p = 0; p < e2; ++p) {
+              acc = kind == 0 ? fmaxf(acc, z[p]) : fminf(acc, z[p]);
+              out[p] = acc;
+            }
+          } else {
+            float acc = z[m - 1];
+            for (int p = m - 1; p >= m - e2; --p) {
+              acc = kind == 2 ? fmaxf(acc, z[p]) : fminf(acc, z[p]);
+              out[p - (m - e2)] = acc;
+            }
+          }
+        }
+      }
+      __syncwarp(gm);
+      // edge layout: [0..3] window i: pu, pl, su, sl; [4..7] window j
+      const EdgeEnv Ei = {edge, edge + lay.e2, edge + 2 * lay.e2, edge + 3 * lay.e2, lay.e2};
+      const EdgeEnv Ej = {edge + 4 * lay.e2, edge + 5 * lay.e2, edge + 6 * lay.e2,
+                          edge + 7 * lay.e2, lay.e2};
+      // ---- LB_Keogh both directions (LB_KK, lb_keogh.cpp:9-72) ----
+      float e1 = 0, m1 = 0, e2s = 0, m2 = 0;
+      for (int k = g; k < m; k += G) {
+        float U, Lw;
+        envelope_at(S, j, mj, sj, Ej, k, &U, &Lw);
+        const float a1 = keogh_term(q[k], U, Lw);
+        envelope_at(S, i, mi, si, Ei, k, &U, &Lw);
+        const float a2 = keogh_term(t[k], U, Lw);
+        if (k < kBias || k >= m - kBias) {
+          e1 += a1;
+          e2s += a2;
+        } else {
+          m1 += a1;
+          m2 += a2;
+        }
+      }
+      e1 = group_sum<G>(e1, gm);
+      m1 = group_sum<G>(m1, gm);
+      e2s = group_sum<G>(e2s, gm);
+      m2 = group_sum<G>(m2, gm);
+      const float lb1 = fmaxf(e1, kl + kr) + m1;
+      const float lb2 = fmaxf(e2s, kl + kr) + m2;
+      if (lb1 > thr || lb2 > thr) {
+        if (g == 0) atomicAdd(&cnt[kPrunedKeogh], 1ull);
+        __syncwarp(gm);
+        continue;
+      }
+      // ---- cumulative bound of the larger direction, 8-cell chunks ----
+      const bool dir1 = lb1 > lb2;
+      for (int x = g; x < lay.nc; x += G) {
+        float acc = 0.0f;
+        for (int k = 8 * x; k < 8 * x + 8 && k < m; ++k) {
+          float v;
+          if (k == 0) v = kl;
+          else if (k == m - kBias) v = kr;
+          else if (k < kBias || k >= m - kBias) v = 0.0f;
+          else {
+            float U, Lw;
+            if (dir1) {
+              envelope_at(S, j, mj, sj, Ej, k, &U, &Lw);
+              v = keogh_term(q[k], U, Lw);
+            } else {
+              envelope_at(S, i, mi, si, Ei, k, &U, &Lw);
+              v = keogh_term(t[k], U, Lw);
+            }
+          }
+          acc += v;
+        }
+        cbc[x] = acc;
+      }
+      __syncwarp(gm);
+      if (g == 0) {
+        float acc = 0.0f;
+        for (int x = lay.nc - 1; x >= 0; --x) {
+          acc += cbc[x];
+          cbc[x] = acc;
+        }
+        cbc[lay.nc] = 0.0f;
+        cbc[lay.nc + 1] = 0.0f;
+      }
+      __syncwarp(gm);
+    }
+    // ---- banded DTW (FP32, early abandoning) ----
+    unsigned long long cells = 0;
+    bool ab = false;
+    const float d2 =
+        dtw_band<float, C, G, true>(q, t, m, w, cbc, lay.nc, thr, Q.bsf2, gm, g, &cells, &ab);
+    if (g == 0) {
+      atomicAdd(&cnt[kDtwCalls], 1ull);
+      atomicAdd(&cnt[kDtwCells], cells);
+      if (ab) {
+        atomicAdd(&cnt[kDtwAbandoned], 1ull);
+      } else {
+        const float now = __uint_as_float(*(volatile unsigned int*)Q.bsf2) * (1.0f + kSlack);
+        if (d2 <= now) {
+          atomicMin(Q.bsf2, __float_as_uint(d2));
+          const unsigned int slot = atomicAdd(Q.cand_count, 1u);
+          if (slot < Q.cand_cap) {
+            Candidate cd;
+            cd.i = (int)i;
+            cd.j = (int)j;
+            cd.d2 = d2;
+            cd.pad = 0;
+            Q.cand[slot] = cd;
+          }
+        }
+      }
+    }
+    __syncwarp(gm);
+  }
+  __syncthreads();
+  for (int x = threadIdx.x; x < kNumCounters; x += blockDim.x)
+    if (cnt[x]) atomicAdd(&Q.counters[x], cnt[x]);
+}
+
+// Exact DTW of a list of pairs (no bounds, no abandoning), FP32 or FP64.
+// With `cands`, pairs come from the candidate list and any candidate above
+// the final best-so-far (plus slack) is skipped with +inf.
+template <typename T, int C, int G>
+__global__ void __launch_bounds__(128) k_dtw_list(DevSeries S, const int2* pairs,
+                                                   const Candidate* cands,
+                                                   const unsigned int* count_ptr, int count,
+                                                   const unsigned int* bsf2, double* out,
+                                                   int group_elems) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
+  const int m = S.m, w = S.w;
+  const int gib = threadIdx.x / G, g = threadIdx.x % G;
+  const unsigned int gm = group_mask<G>();
+  const int groups = blockDim.x / G;
+  const int pq = G + 1, pt = G * C + G + 2;
+  T* q = sm + (size_t)gib * group_elems + pq;
+  T* t = q + m + pq + pt;
+  for (int x = g; x < pq; x += G) {
+    q[-1 - x] = Pad<T>::q();
+    q[m + x] = Pad<T>::q();
+  }
+  for (int x = g; x < pt; x += G) {
+    t[-1 - x] = Pad<T>::t();
+    t[m + x] = Pad<T>::t();
+  }
+  __syncwarp(gm);
+  int n = count;
+  if (count_ptr) {
+    const unsigned int c = *count_ptr;
+    n = (int)(c < (unsigned)count ? c : (unsigned)count);
+  }
+  const float fin = bsf2 ? __uint_as_float(*bsf2) * (1.0f + kSlack) : 0.0f;
+  for (int k = blockIdx.x * groups + gib; k < n; k += gridDim.x * groups) {
+    int64_t i, j;
+    if (cands) {
+      const Candidate cd = cands[k];
+      i = cd.i;
+      j = cd.j;
+      if (bsf2 && cd.d2 > fin) {
+        if (g == 0) out[k] = __longlong_as_double(0x7ff0000000000000LL);
+        continue;
+      }
+    } else {
+      i = pairs[k].x;
+      j = pairs[k].y;
+    }
+    const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
+    for (int x = g; x < m; x += G) {
+      q[x] = (T)((S.a[i + x] - mi) * si);
+      t[x] = (T)((S.a[j + x] - mj) * sj);
+    }
+    __syncwarp(gm);
+    unsigned long long cells;
+    bool ab;
+    const T d2 = dtw_band<T, C, G, false>(q, t, m, w, nullptr, 0, 0.0f, nullptr, gm, g, &cells,
+                                         &ab);
+    if (g == 0) out[k] = (double)d2;
+    __syncwarp(gm);
+  }
+}
+
+// Lexicographic minimum (d2, i, j) over the verified candidates.
+__global__ void k_best(const Candidate* cands, const unsigned int* count_ptr, int cap,
+                       const double* d2, double* out_d2, int* out_idx) {
+  const unsigned int c = *count_ptr;
+  const int n = (int)(c < (unsigned)cap ? c : (unsigned)cap);
+  __shared__ double bd[32];
+  __shared__ int bk[32];
+  const double INF = __longlong_as_double(0x7ff0000000000000LL);
+  double best = INF;
+  int bi = -1;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const double v = d2[k];
+    if (!(v < INF)) continue;
+    if (bi < 0 || v < best ||
+        (v == best && (cands[k].i < cands[bi].i ||
+                       (cands[k].i == cands[bi].i && cands[k].j < cands[bi].j)))) {
+      best = v;
+      bi = k;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+    const int ok = __shfl_xor_sync(0xffffffffu, bi, o);
+    bool take = false;
+    if (ok >= 0) {
+      if (bi < 0 || ov < best) take = true;
+      else if (ov == best && (cands[ok].i < cands[bi].i ||
+                              (cands[ok].i == cands[bi].i && cands[ok].j < cands[bi].j)))
+        take = true;
+    }
+    if (take) {
+      best = ov;
+      bi = ok;
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    bd[threadIdx.x >> 5] = best;
+    bk[threadIdx.x >> 5] = bi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = __longlong_as_double(0x7ff0000000000000LL);
+    int k = -1;
+    for (int x = 0; x < (int)(blockDim.x >> 5); ++x) {
+      const int ok = bk[x];
+      if (ok < 0) continue;
+      const double ov = bd[x];
+      if (k < 0 || ov < b ||
+          (ov == b && (cands[ok].i < cands[k].i ||
+                       (cands[ok].i == cands[k].i && cands[ok].j < cands[k].j)))) {
+        b = ov;
+        k = ok;
+      }
+    }
+    *out_d2 = b;
+    *out_idx = k;
+  }
+}
+
+// ---- dispatch ----
+
+template <int C, int G>
+void run_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
+               const unsigned int* npairs, int flags, int num_sms, cudaStream_t st) {
+  const bool bounds = flags & 1;
+  const GroupLayout lay = group_layout(S.m, S.w, C, G, bounds);
+  const int groups = 128 / G;
+  size_t bytes = (size_t)groups * lay.total * sizeof(float);
+  int threads = 128;
+  // keep at least two blocks per SM when the series is long
+  while (bytes > 100 * 1024 && threads > G && threads > 32) {
+    threads /= 2;
+    bytes /= 2;
+  }
+  const int gpb = threads / G;
+  bytes = (size_t)gpb * lay.total * sizeof(float);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_pairs<C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    configured = true;
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs<C, G>, threads, bytes);
+  if (per_sm < 1) per_sm = 1;
+  k_pairs<C, G><<<num_sms * per_sm, threads, bytes, st>>>(S, Q, pairs, npairs, flags, lay.total);
+}
+
+template <typename T, int C, int G>
+void run_list(const DevSeries& S, const int2* pairs, const Candidate* cands,
+              const unsigned int* count_ptr, int count, const unsigned int* bsf2, double* out,
+              cudaStream_t st) {
+  const int pq = G + 1, pt = G * C + G + 2;
+  const int elems = ((2 * pq + 2 * pt + 2 * S.m) + 3) & ~3;
+  int threads = 128;
+  size_t bytes = (size_t)(threads / G) * elems * sizeof(T);
+  while (bytes > 100 * 1024 && threads > G && threads > 32) {
+    threads /= 2;
+    bytes /= 2;
+  }
+  bytes = (size_t)(threads / G) * elems * sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_dtw_list<T, C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    configured = true;
+  }
+  const int groups = threads / G;
+  int blocks = (count + groups - 1) / groups;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_dtw_list<T, C, G><<<blocks, threads, bytes, st>>>(S, pairs, cands, count_ptr, count, bsf2,
+                                                      out, elems);
+}
+
+#define DTWJ_BAND_CASES(X) \
+  X(2, 4) X(3, 4) X(4, 4) X(5, 4) X(6, 4) X(7, 4) X(8, 4) \
+  X(2, 8) X(3, 8) X(4, 8) X(5, 8) X(6, 8) X(7, 8) X(8, 8) \
+  X(2, 16) X(3, 16) X(4, 16) X(5, 16) X(6, 16) X(7, 16) X(8, 16) \
+  X(2, 32) X(3, 32) X(4, 32) X(5, 32) X(6, 32) X(7, 32) X(8, 32) \
+  X(10, 32) X(12, 32) X(16, 32)
+
+bool band_supported(int C, int G) {
+#define X(c, g) if (C == c && G == g) return true;
+  DTWJ_BAND_CASES(X)
+#undef X
+  return false;
+}
+
+}  // namespace
+
+bool choose_band(int w, BandShape* out) {
+  const int cells = 2 * w + 1;
+  const int Gs[4] = {32, 16, 8, 4};
+  double best = 2.0;
+  BandShape pick = {0, 0};
+  for (int gi = 0; gi < 4; ++gi) {
+    const int G = Gs[gi];
+    int C = (cells + G - 1) / G;
+    if (C < 2) C = 2;
+    while (C <= 16 && !band_supported(C, G)) ++C;
+    if (C > 16) continue;
+    const double waste = (double)(G * C - cells) / (double)(G * C);
+    if (waste < best - 1e-9) {
+      best = waste;
+      pick.C = C;
+      pick.G = G;
+    }
+  }
+  if (pick.G == 0) return false;
+  *out = pick;
+  return true;
+}
+
+void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
+                  const unsigned int* npairs, bool masked, bool bounds, BandShape band,
+                  int num_sms, cudaStream_t st) {
+  const int flags = (bounds ? 1 : 0) | (masked ? 2 : 0);
+#define X(c, g) \
+  if (band.C == c && band.G == g) { run_pairs<c, g>(S, Q, pairs, npairs, flags, num_sms, st); return; }
+  DTWJ_BAND_CASES(X)
+#undef X
+}
+
+void launch_verify(const DevSeries& S, const DevSearch& Q, BandShape band, double* out_d2,
+                   double* best_d2, int* best_idx, cudaStream_t st) {
+#define X(c, g)                                                                          \
+  if (band.C == c && band.G == g) {                                                      \
+    run_list<double, c, g>(S, nullptr, Q.cand, Q.cand_count, (int)Q.cand_cap, Q.bsf2,   \
+                           out_d2, st);                                                  \
+  }
+  DTWJ_BAND_CASES(X)
+#undef X
+  k_best<<<1, 256, 0, st>>>(Q.cand, Q.cand_count, (int)Q.cand_cap, out_d2, best_d2, best_idx);
+}
+
+void launch_pair_dtw(const DevSeries& S, const int2* pairs, int count, bool precise,
+                     BandShape band, double* out_d2, cudaStream_t st) {
+#define X(c, g)                                                                       \
+  if (band.C == c && band.G == g) {                                                   \
+    if (precise)                                                                      \
+      run_list<double, c, g>(S, pairs, nullptr, nullptr, count, nullptr, out_d2, st); \
+    else                                                                              \
+      run_list<float, c, g>(S, pairs, nullptr, nullptr, count, nullptr, out_d2, st);  \
+  }
+  DTWJ_BAND_CASES(X)
+#undef X
+}
+
+}  // namespace dtwj

@@ -1,0 +1,135 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's golden
+outputs and with the oracle.  Tolerances: top-1 indices bit-exact; distance
+within 1e-5 relative of the FP64 reference / oracle (the device search runs
+in FP32 and re-verifies its final candidates in FP64)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG_DIR
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-5
+
+
+def _check(r, i, j, dist, what=""):
+    assert (r.i, r.j) == (i, j), what
+    assert abs(r.dist - dist) <= REL * max(dist, 1e-12), (what, r.dist, dist)
+
+
+def test_golden_reference_joins(gpu_dtwj, golden):
+    for c in golden:
+        r = gpu_dtwj.join(c["series"], c["m"], c["w"])
+        _check(r, c["i"], c["j"], c["dist"], c["name"])
+        s = r.n - r.m + 1
+        assert r.pairs == (s - r.m) * (s - r.m + 1) // 2  # every pair with j - i >= m
+
+
+@pytest.mark.parametrize("n,m,w,seed,kind", [
+    (2000, 16, 1, 1, "rw"), (2500, 32, 2, 2, "rw"), (3000, 64, 3, 3, "rw"),
+    (3000, 64, 13, 4, "ecg"), (4000, 128, 26, 5, "rw"), (3500, 100, 52, 6, "rw"),
+    (5000, 256, 103, 7, "rw"), (4000, 300, 103, 8, "ecg"), (3000, 40, 40, 9, "rw"),
+    (2600, 24, 70, 10, "rw"),
+])
+def test_join_matches_oracle(gpu_dtwj, oracle, synth, n, m, w, seed, kind):
+    x = synth.random_walk(n, seed) if kind == "rw" else synth.ecg_like(n, seed)
+    ref = oracle.join(x, m, min(w, m - 1))
+    r = gpu_dtwj.join(x, m, w)
+    _check(r, ref.i, ref.j, ref.dist, (n, m, w))
+
+
+def test_flags_do_not_change_the_result(gpu_dtwj, golden):
+    c = [g for g in golden if g["name"] == "rw6k_m128_w6"][0]
+    base = gpu_dtwj.join(c["series"], c["m"], c["w"])
+    for fl in (gpu_dtwj.F_NO_MASKED, gpu_dtwj.F_NO_SEED, gpu_dtwj.F_NO_DIAG,
+               gpu_dtwj.F_NO_SEED | gpu_dtwj.F_NO_MASKED):
+        r = gpu_dtwj.join(c["series"], c["m"], c["w"], fl)
+        assert (r.i, r.j, r.dist) == (base.i, base.j, base.dist), fl
+    nd = gpu_dtwj.join(c["series"], c["m"], c["w"], gpu_dtwj.F_NO_DIAG)
+    assert nd.pruned_fast == 0 and nd.pairs == base.pairs
+
+
+def test_deterministic(gpu_dtwj, golden):
+    c = golden[0]
+    a = gpu_dtwj.join(c["series"], c["m"], c["w"])
+    b = gpu_dtwj.join(c["series"], c["m"], c["w"])
+    assert (a.i, a.j, a.dist) == (b.i, b.j, b.dist)
+
+
+def test_pair_dtw_matches_oracle(gpu_dtwj, oracle, synth):
+    x = synth.random_walk(6000, 31)
+    rng = np.random.default_rng(5)
+    for m, w in [(16, 1), (64, 3), (128, 13), (256, 26), (512, 52), (300, 103), (50, 60)]:
+        pi = rng.integers(0, x.size - m + 1, 40)
+        pj = rng.integers(0, x.size - m + 1, 40)
+        d64 = gpu_dtwj.pair_dtw(x, m, w, pi, pj, precise=True)
+        d32 = gpu_dtwj.pair_dtw(x, m, w, pi, pj, precise=False)
+        ref = np.array([oracle.pair_dist(x, m, min(w, m - 1), int(a), int(b))
+                        for a, b in zip(pi, pj)])
+        np.testing.assert_allclose(d64, ref, rtol=1e-10)
+        np.testing.assert_allclose(d32, ref, rtol=2e-4)
+
+
+def test_matrix_profile_matches_oracle(gpu_dtwj, oracle, synth):
+    x = synth.random_walk(5000, 41)
+    m = 64
+    mp, mpi = gpu_dtwj.matrix_profile(x, m)
+    omp, ompi = oracle.mp(x, m)
+    np.testing.assert_allclose(mp, omp, rtol=1e-6, atol=1e-6)
+    assert np.mean(mpi == ompi) > 0.999
+
+
+def test_nan_input_is_rejected(gpu_dtwj, synth):
+    x = synth.random_walk(3000, 1)
+    x[77] = np.nan
+    with pytest.raises(gpu_dtwj.DtwjError) as e:
+        gpu_dtwj.join(x, 64, 3)
+    assert e.value.code == gpu_dtwj.ERR_NAN
+
+
+def test_flat_windows_are_excluded(gpu_dtwj, oracle, synth):
+    x = synth.random_walk(3000, 7)
+    x[1000:1200] = 5.0
+    ref = oracle.join(x, 64, 4)
+    r = gpu_dtwj.join(x, 64, 4)
+    _check(r, ref.i, ref.j, ref.dist)
+
+
+def test_exact_duplicate_resolves_to_lowest_index(gpu_dtwj, synth):
+    x = synth.random_walk(3000, 8)
+    seg = x[400:480].copy()
+    x[1200:1280] = seg
+    x[2200:2280] = seg
+    r = gpu_dtwj.join(x, 80, 4)
+    assert (r.i, r.j) == (400, 1200) and r.dist == 0.0
+
+
+def test_context_reuse_and_batch(gpu_dtwj, golden):
+    cs = golden[:4]
+    with gpu_dtwj.Context() as ctx:
+        for c in cs:
+            r = ctx.join(c["series"], c["m"], c["w"])
+            _check(r, c["i"], c["j"], c["dist"], c["name"])
+    rs = gpu_dtwj.join_batch([c["series"] for c in cs], [c["m"] for c in cs],
+                             [c["w"] for c in cs])
+    for r, c in zip(rs, cs):
+        _check(r, c["i"], c["j"], c["dist"], c["name"])
+
+
+def test_cli_drop_in(tmp_path, golden):
+    c = [g for g in golden if g["name"] == "rw20k"][0]
+    data = tmp_path / "rw20k.txt"
+    np.savetxt(data, c["series"], fmt="%.17g")
+    tf = tmp_path / "time.txt"
+    tf.write_text("1.5\n")
+    cli = os.path.join(PKG_DIR, "bin", "dtwj")
+    # ratio 0.01 at m=256 -> w = ceil(2.56) = 3, the fixture's band
+    out = subprocess.run([cli, str(data), str(tf), "256", "0.01"], capture_output=True,
+                         text=True, check=True).stdout
+    assert "first min is %d sec min is %d" % (c["i"] + 1, c["j"] + 1) in out
+    assert "final distance :%f" % c["dist"] in out
+    lines = tf.read_text().splitlines()
+    assert len(lines) == 2 and lines[0] == "1.5" and float(lines[1]) > 0
