@@ -253,6 +253,7 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
     CUDA_OK(cudaMemsetAsync(nseeds + 1, 0, 4, st));
     DevSearch Qs = Q;
     Qs.queue_next = nseeds + 1;
+    Qs.queue_cap = kSeeds;
     launch_pairs(S, Qs, seeds, nseeds, masked, false, band, ctx->num_sms, st);
     unsigned int b2 = 0;
     CUDA_OK(cudaMemcpyAsync(&b2, Q.bsf2, 4, cudaMemcpyDeviceToHost, st));

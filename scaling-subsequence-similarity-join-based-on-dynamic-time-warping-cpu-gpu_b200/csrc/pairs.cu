@@ -134,12 +134,20 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
       for (int c = 0; c < C; ++c)
         if (c == c0) result = cur[c];
     }
+    if (tau < G) {
+      // warm-up: a lane that has not reached row 0 keeps its initial row
+      // (which holds the virtual start D(-1, 0) = 0 for the lane owning d = 0)
+      const bool live = r >= 0;
 #pragma unroll
-    for (int c = 0; c < C; ++c) prev[c] = cur[c];
+      for (int c = 0; c < C; ++c) prev[c] = live ? cur[c] : prev[c];
+    } else {
+#pragma unroll
+      for (int c = 0; c < C; ++c) prev[c] = cur[c];
+    }
 #pragma unroll
     for (int c = 0; c < C - 1; ++c) tw[c] = tw[c + 1];
     tw[C - 1] = t[r + d_lo + C];
-    if (ABANDON && (tau & 15) == 15 && tau < tau_end) {
+    if (ABANDON && (tau & 15) == 15 && tau >= G && tau < tau_end) {
       T fm = cur[0];
 #pragma unroll
       for (int c = 1; c < C; ++c) fm = fmin_(fm, cur[c]);
@@ -261,7 +269,7 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
     t[m + x] = kPadT;
   }
   __syncthreads();
-  const unsigned int total = *npairs;
+  const unsigned int total = *npairs < Q.queue_cap ? *npairs : Q.queue_cap;
   for (;;) {
     unsigned int idx = 0;
     if (g == 0) idx = atomicAdd(Q.queue_next, 1u);
