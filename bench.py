@@ -1,0 +1,381 @@
+#!/usr/bin/env python3
+"""Benchmark of the top-1 z-normalised DTW subsequence self-join.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+Workload (default): one float64 random walk, n = 1,000,000, seed 1, with one
+planted motif pair (length-1024 sum of 3 sines, N(0, 0.1) noise, +-5 % time
+warp), m = 1024, ratio 0.05 -> w = 52.  A step is one complete join of that
+series (ED profile, seeds, diagonal sweep, per-pair bounds, DTW, FP64
+verification).  The metric is join throughput in candidate pairs per second
+(every pair (i, j) with j - i >= m counts once); join time and DTW cells/s
+ride along.
+
+Timing: W untimed warm-up joins, then exactly K joins bracketed by a
+synchronize; `value` uses the device time the library measures with CUDA
+events on its own stream (inputs resident in HBM).  `e2e` repeats the join
+through the public host-pointer API from pinned memory, so the H2D copy of
+the series and the D2H read of the result are inside the timed region.  The
+series (8 MB) and the per-series arrays (~250 MB) are re-read from HBM on
+every join; the sweep's working set far exceeds what one join leaves in L2.
+
+--impl reference times the reference's own CPU implementation (CPU_version1,
+built from its sources into oracle/_ref/) on bounded samples of the same
+series, one single-threaded process per host core.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "Join time & DTW cells/s, n=1M m=1024 r=0.05: learned-order vs plain GPU, exact"
+UNIT = "pairs/s"
+
+
+def _load_pkg():
+    from conftest import load_package, load_synth  # path helpers only
+    return load_package(), load_synth()
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured", d.get("sm_max_mhz", 1965.0)
+    return 6650.0, "fallback", 1965.0
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local, dist
+
+
+def _max_over_ranks(v: float, dist, local: int) -> float:
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda:%d" % local)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_sample_reference(x: np.ndarray, m: int, w: int, n_sample: int, procs: int):
+    """Runs the reference CPU join (oracle/_ref/ref_join) on `procs` disjoint
+    samples of length n_sample in parallel; returns (pairs/s, per-run info)."""
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "ref_join")
+    if not os.path.exists(ref_bin):
+        return None
+    files = []
+    tmp = tempfile.mkdtemp(prefix="dtwj_ref_")
+    for k in range(procs):
+        lo = (k * n_sample) % max(1, x.size - n_sample)
+        path = os.path.join(tmp, "s%d.f64" % k)
+        x[lo:lo + n_sample].astype("<f8").tofile(path)
+        files.append(path)
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen([ref_bin, f, str(m), str(w)], stdout=subprocess.PIPE,
+                           stderr=subprocess.DEVNULL, text=True) for f in files]
+    outs = [p.communicate()[0] for p in ps]
+    wall = time.perf_counter() - t0
+    s = n_sample - m + 1
+    pairs = (s - m) * (s - m + 1) // 2
+    runs = []
+    for o in outs:
+        try:
+            line = o.strip().splitlines()[-1].replace(": -nan", ": null").replace(": nan", ": null")
+            runs.append(json.loads(line))
+        except (IndexError, json.JSONDecodeError):
+            pass
+    return pairs * len(files) / wall, wall, pairs, runs
+
+
+def cpu_sample_port(x: np.ndarray, m: int, w: int, n_sample: int, threads: int):
+    """The oracle's C restatement (OpenMP) on one sample; returns pairs/s."""
+    from conftest import Oracle, ORACLE_LIB
+    if not os.path.exists(ORACLE_LIB):
+        return None
+    orc = Oracle()
+    y = np.ascontiguousarray(x[:n_sample])
+    t0 = time.perf_counter()
+    r = orc.join(y, m, w, threads=threads)
+    wall = time.perf_counter() - t0
+    return r.pairs / wall, wall, r.pairs, r.threads
+
+
+def run_reference_arm(args):
+    world, rank, local, dist = int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("RANK", "0")), 0, None
+    if rank != 0:
+        return 0
+    _, synth = _load_pkg()
+    wl = synth.workload(args.workload)
+    x, m, w = wl["series"], wl["m"], wl["w"]
+    cores = os.cpu_count() or 1
+    n_sample = args.ref_sample
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_join")):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/ref_join not built (needs the reference "
+                                         "sources: oracle/build_ref.sh)"}))
+        return 0
+    for _ in range(args.warmup):
+        cpu_sample_reference(x, m, w, n_sample, cores)
+    vals, walls = [], []
+    for _ in range(args.steps):
+        v, wall, pairs, runs = cpu_sample_reference(x, m, w, n_sample, cores)
+        vals.append(v)
+        walls.append(wall)
+    value = sum(vals) / len(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(walls) / len(walls),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload + " sampled", "n": int(n_sample), "m": m, "w": w,
+                   "processes": cores},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": "%d x first-%d-sample slices of the series, one "
+                                   "CPU_version1 DTWMotifDiscoveryGUI (mpx_v2 + join) per "
+                                   "process" % (cores, n_sample)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    world, rank, local, dist = _dist_init()
+    dtwj, synth = _load_pkg()
+    wl = synth.workload(args.workload)
+    x, m, w = wl["series"], wl["m"], wl["w"]
+    n = x.size
+    s = n - m + 1
+    pairs_total = (s - m) * (s - m + 1) // 2
+    try:
+        import torch
+        have_torch = torch.cuda.is_available()
+    except ImportError:
+        have_torch = False
+    if have_torch:
+        torch.cuda.set_device(local)
+        xd = torch.from_numpy(x).to("cuda:%d" % local)
+        xh = torch.from_numpy(x).pin_memory()
+        dptr, hptr = xd.data_ptr(), xh.data_ptr()
+    else:
+        raise SystemExit("bench.py needs torch with CUDA for device buffers")
+    ctx = dtwj.Context(local)
+    flags = 0
+    for _ in range(args.warmup):
+        ctx.join_device(dptr, n, m, w, flags)
+    _barrier(dist)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    results = [ctx.join_device(dptr, n, m, w, flags) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    dev_seconds = sum(r.seconds_join for r in results)
+    dev_seconds = _max_over_ranks(dev_seconds, dist, local)
+    r0 = results[-1]
+    value = world * pairs_total * args.steps / dev_seconds
+
+    # profiled pass: per-phase device time for the roofline (same workload)
+    prof = ctx.join_device(dptr, n, m, w, flags | dtwj.F_PROFILE)
+    phases = dict(zip(dtwj.PHASES, prof.phase_seconds[:len(dtwj.PHASES)]))
+    launches = dict(zip(dtwj.PHASES, prof.phase_launches[:len(dtwj.PHASES)]))
+    dominant = max(phases, key=phases.get)
+
+    # e2e through the host-pointer API (pinned host buffer)
+    fn = dtwj.load().dtwj_ctx_join
+    R = dtwj._Result
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        rr = R()
+        rc = fn(ctx._h, ctypes.cast(ctypes.c_void_p(hptr), ctypes.POINTER(ctypes.c_double)),
+                n, m, w, flags, ctypes.byref(rr))
+        assert rc == 0, dtwj.strerror(rc)
+    torch.cuda.synchronize()
+    e2e_wall = _max_over_ranks(time.perf_counter() - t1, dist, local)
+
+    hbm_peak, peak_kind, sm_max = _peaks()
+    # algorithmic bytes of the diagonal sweep: every tile streams its row and
+    # column slices of the per-index arrays once (8 FP64 row/column arrays for
+    # the fast bound + mask/series/envelope slices of the masked bound).
+    tiles_rows = 0
+    for L0 in range(m, s, 128):
+        rows = s - L0
+        tiles_rows += rows + (rows + 4095) // 4096 * 128
+    bytes_per_index = 8 * 8 + (4 + 8 + 8) * 2
+    diag_bytes = tiles_rows * 2 * bytes_per_index
+    diag_launches = max(1, launches["diag"])
+    per_launch_s = phases["diag"] / diag_launches
+    achieved_gbs = diag_bytes / max(phases["diag"], 1e-12) / 1e9
+    fp64_flops = pairs_total * 32.0  # 8 FP64 accumulators x 2 DFMA per pair
+    fp64_peak = 148 * 64 * 2 * sm_max * 1e6 / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "diag_sweep_traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get("bytes_per_launch_scaled")
+    cells_per_s = r0.dtw_cells / max(phases.get("pairs", 1e-12) + phases.get("seeds", 0), 1e-12)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        got = cpu_sample_reference(x, m, w, args.cpu_sample, 1)
+        if got is not None:
+            v, cw, p, runs = got
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "first %d samples of the series, m=%d w=%d, CPU_version1 "
+                             "DTWMotifDiscoveryGUI (mpx_v2 + join), %d pairs in %.1f s"
+                             % (args.cpu_sample, m, w, p, cw)}
+        else:
+            got = cpu_sample_port(x, m, w, args.cpu_sample, 1)
+            if got is not None:
+                v, cw, p, th = got
+                cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
+                       "sample": "first %d samples, oracle C restatement, %.1f s"
+                                 % (args.cpu_sample, cw)}
+    gpu_launches = int(sum(prof.phase_launches[:len(dtwj.PHASES)])) * args.steps
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * dev_seconds / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+        "data": "synthetic (seeded random walk + planted motif)",
+        "config": {"workload": args.workload, "n": n, "m": m, "w": w,
+                   "pairs_per_join": pairs_total, "l2": "inputs+working set > L2 per join",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "join_seconds": dev_seconds / args.steps,
+        "result": {"i": r0.i, "j": r0.j, "dist": r0.dist},
+        "pruned": {"fast": r0.pruned_fast, "masked": r0.pruned_masked, "kim": r0.pruned_kim,
+                   "keogh": r0.pruned_keogh, "dtw_calls": r0.dtw_calls,
+                   "dtw_abandoned": r0.dtw_abandoned},
+        "dtw_cells_per_s": cells_per_s,
+        "phase_seconds": phases,
+        "roofline": {"bound": "hbm", "kernel": "diag sweep (k_lb)", "achieved": achieved_gbs,
+                     "peak": hbm_peak, "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "per_launch_ms": 1000 * per_launch_s},
+        "issue_roofline": {"pipe": "fp64", "kernel": "diag sweep (k_lb)",
+                           "achieved": fp64_flops / max(phases["diag"], 1e-12) / 1e12,
+                           "peak": fp64_peak, "unit": "TFLOP/s",
+                           "frac": fp64_flops / max(phases["diag"], 1e-12) / 1e12 / fp64_peak,
+                           "peak_kind": "nominal 148 SM x 64 DFMA/clk x max clock"},
+        "dominant_phase": dominant,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * pairs_total * args.steps / e2e_wall, "unit": UNIT,
+                "h2d_bytes_per_step": int(x.nbytes), "d2h_bytes_per_step": 360},
+        "gpu_launches": gpu_launches,
+        "clocks": clk,
+        "wall_seconds_timed": wall,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rw1m_motif")
+    ap.add_argument("--cpu-sample", type=int, default=16384)
+    ap.add_argument("--ref-sample", type=int, default=8192)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

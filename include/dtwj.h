@@ -55,6 +55,16 @@ extern "C" {
 #define DTWJ_F_NO_DIAG 0x4u     /* skip all diagonal bounds (LB_Keogh + DTW)  */
 #define DTWJ_F_LEARNED 0x8u     /* order the tile queue with the loaded MLP   */
 #define DTWJ_F_VERBOSE 0x10u    /* phase timings on stderr                    */
+#define DTWJ_F_PROFILE 0x20u    /* per-phase device times (CUDA events)       */
+
+/* phases reported in dtwj_result.phase_seconds / phase_launches */
+#define DTWJ_PHASE_PREP 0       /* statistics, envelopes, mask, row terms     */
+#define DTWJ_PHASE_PROFILE 1    /* ED matrix profile                          */
+#define DTWJ_PHASE_SEEDS 2      /* seed selection and seed DTWs               */
+#define DTWJ_PHASE_DIAG 3       /* diagonal bound sweep                       */
+#define DTWJ_PHASE_PAIRS 4      /* endpoint / LB_Keogh / DTW on survivors     */
+#define DTWJ_PHASE_VERIFY 5     /* FP64 re-verification                       */
+#define DTWJ_NUM_PHASES 6
 
 typedef struct {
   int64_t i, j;            /* top-1 pair, 0-based, j - i >= m                */
@@ -74,6 +84,8 @@ typedef struct {
   double seconds_total;    /* wall time of the call                          */
   int64_t n;
   int32_t m, w;
+  double phase_seconds[8];   /* with DTWJ_F_PROFILE: device time per phase   */
+  uint64_t phase_launches[8];/* kernel launches per phase                    */
 } dtwj_result;
 
 typedef struct dtwj_ctx dtwj_ctx;

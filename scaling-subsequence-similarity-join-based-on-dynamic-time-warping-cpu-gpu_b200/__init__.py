@@ -39,6 +39,9 @@ F_NO_SEED = 0x2
 F_NO_DIAG = 0x4
 F_LEARNED = 0x8
 F_VERBOSE = 0x10
+F_PROFILE = 0x20
+
+PHASES = ("prep", "profile", "seeds", "diag", "pairs", "verify")
 
 # Every symbol include/dtwj.h declares.
 EXPORTS = (
@@ -83,6 +86,8 @@ class _Result(ctypes.Structure):
         ("n", ctypes.c_int64),
         ("m", ctypes.c_int32),
         ("w", ctypes.c_int32),
+        ("phase_seconds", ctypes.c_double * 8),
+        ("phase_launches", ctypes.c_uint64 * 8),
     ]
 
 
@@ -107,10 +112,16 @@ class JoinResult:
     n: int
     m: int
     w: int
+    phase_seconds: list
+    phase_launches: list
 
     @staticmethod
     def _from(r: _Result) -> "JoinResult":
-        return JoinResult(**{name: getattr(r, name) for name, _ in _Result._fields_})
+        d = {}
+        for name, _ in _Result._fields_:
+            v = getattr(r, name)
+            d[name] = list(v) if name.startswith("phase_") else v
+        return JoinResult(**d)
 
 
 _lib = None

@@ -79,6 +79,8 @@ struct DevSeries {
   float* MN;        // s, sum_T M (nU^2 + nL^2)
   float* MDUL2;     // s, sum_m M (nU - nL)^2
   float* MDUL;      // s
+  double* SM;       // s, sum_T M            (T = [kBias, m-1-kBias])
+  double* SME;      // s, sum_T M E
   int* status;      // device status word (0 ok, else error bits)
 };
 
@@ -94,6 +96,34 @@ struct DevSearch {
   unsigned int* queue_next;
   unsigned int queue_cap;
 };
+
+// Endpoint bound: minimum cost of any warping path's cells in the first and
+// last three layers (LB_KIM, CPU_version1/lb_kim.cpp:10-73).  q = window i,
+// t = window j (any indexable sequences); cells are (t index, q index).  The
+// reference's fourth option adds the corner cell twice (lb_kim.cpp:55,62);
+// here it is added once so that the bound stays admissible.
+template <typename V, typename Seq>
+__device__ __forceinline__ void kim_bound(const Seq& q, const Seq& t, int m, V* left, V* right) {
+  auto D2 = [](V x, V y) { return (x - y) * (x - y); };
+  auto mn = [](V x, V y) { return x < y ? x : y; };
+  const V o = D2(t[0], q[0]);
+  const V lw = mn(D2(t[1], q[0]), D2(t[1], q[1]));
+  const V l1 = mn(lw, D2(t[0], q[1]));
+  V d = mn(D2(t[1], q[0]) + D2(t[2], q[0]), lw + D2(t[2], q[1]));
+  d = mn(d, D2(q[1], t[1]) + D2(q[2], t[2]));
+  d = mn(d, l1 + D2(q[2], t[1]));
+  d = mn(d, D2(q[1], t[0]) + D2(q[2], t[0]));
+  *left = o + d;
+  const int e = m - 1;
+  const V o2 = D2(t[e], q[e]);
+  const V rw = mn(D2(t[e - 1], q[e]), D2(t[e - 1], q[e - 1]));
+  const V r1 = mn(rw, D2(t[e], q[e - 1]));
+  d = mn(D2(t[e - 1], q[e]) + D2(t[e - 2], q[e]), rw + D2(t[e - 2], q[e - 1]));
+  d = mn(d, D2(q[e - 1], t[e - 1]) + D2(q[e - 2], t[e - 2]));
+  d = mn(d, r1 + D2(q[e - 2], t[e - 1]));
+  d = mn(d, D2(q[e - 1], t[e]) + D2(q[e - 2], t[e]));
+  *right = o2 + d;
+}
 
 struct BandShape {
   int C;  // cells (diagonals) per lane
@@ -118,12 +148,14 @@ void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
                         cudaStream_t st);
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
                         unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st);
-// enumerate_all: no pruning, every pair goes to the queue (bounds disabled)
+// masked: evaluate the masked bound; enumerate_all: no pruning, every pair
+// goes to the queue (diagonal bounds disabled)
 void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
-               int tile_end, bool enumerate_all, cudaStream_t st);
+               int tile_end, bool masked, bool enumerate_all, cudaStream_t st);
+// bounds = false: DTW only (the seeds); true: endpoint bound + LB_Keogh first
 void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
-                  const unsigned int* npairs, bool masked, bool bounds, BandShape band,
-                  int num_sms, cudaStream_t st);
+                  const unsigned int* npairs, bool bounds, BandShape band, int num_sms,
+                  cudaStream_t st);
 void launch_verify(const DevSeries& S, const DevSearch& Q, BandShape band, double* out_d2,
                    double* best_d2, int* best_idx, cudaStream_t st);
 void launch_pair_dtw(const DevSeries& S, const int2* pairs, int count, bool precise,

@@ -55,13 +55,14 @@ struct dtwj_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<Tile> tiles_host;
   int64_t tiles_n = -1, tiles_m = -1;
+  std::vector<cudaEvent_t> pool;  // events for per-phase device times
 };
 
 namespace {
 
 enum BufId {
   B_A = 0, B_MU, B_SIG, B_ISG, B_FLAT, B_U, B_L, B_E, B_NU, B_DFA, B_DGA, B_DFE, B_DGE,
-  B_AC, B_DUL, B_QSIG, B_MASK, B_MN, B_MDUL2, B_MDUL, B_STATUS,
+  B_AC, B_DUL, B_QSIG, B_MASK, B_MN, B_MDUL2, B_MDUL, B_SM, B_SME, B_STATUS,
   B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_KEYS_LO, B_TILES, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
   B_MP, B_MPI,
@@ -104,6 +105,49 @@ int ensure(dtwj_ctx* c, int id, size_t bytes, void** out) {
     }                                                                 \
   } while (0)
 
+// Per-phase device time from CUDA events recorded on the join's stream
+// (DTWJ_F_PROFILE); a no-op otherwise.
+struct Phases {
+  dtwj_ctx* ctx;
+  bool on;
+  size_t used = 0;
+  struct Mark {
+    int phase;
+    size_t a, b;
+    int launches;
+  };
+  std::vector<Mark> marks;
+  size_t open_at = 0;
+  Phases(dtwj_ctx* c, bool enabled) : ctx(c), on(enabled) {}
+  cudaEvent_t ev(size_t k) {
+    while (ctx->pool.size() <= k) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ctx->pool.push_back(e);
+    }
+    return ctx->pool[k];
+  }
+  void begin() {
+    if (!on) return;
+    open_at = used;
+    cudaEventRecord(ev(used++), ctx->stream);
+  }
+  void end(int phase, int launches) {
+    if (!on) return;
+    cudaEventRecord(ev(used), ctx->stream);
+    marks.push_back({phase, open_at, used, launches});
+    ++used;
+  }
+  void collect(dtwj_result* out) {
+    for (auto& mk : marks) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ctx->pool[mk.a], ctx->pool[mk.b]);
+      out->phase_seconds[mk.phase] += ms / 1000.0;
+      out->phase_launches[mk.phase] += (uint64_t)mk.launches;
+    }
+  }
+};
+
 int check_args(const void* x, int64_t n, int32_t m, int32_t w) {
   if (!x || m < 8 || w < 0) return DTWJ_ERR_ARG;
   if (n < 2 * (int64_t)m + 1 || n > (int64_t)INT32_MAX - 4) return DTWJ_ERR_ARG;
@@ -132,7 +176,7 @@ void build_tiles(dtwj_ctx* ctx, int64_t n, int m) {
 
 // Allocates and prepares every per-series array; returns the DevSeries.
 int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool masked,
-            DevSeries* out) {
+            DevSeries* out, Phases* ph = nullptr) {
   const int64_t s = n - m + 1;
   DevSeries S;
   memset(&S, 0, sizeof S);
@@ -160,6 +204,8 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   ENSURE(B_MN, s * 4, S.MN);
   ENSURE(B_MDUL2, s * 4, S.MDUL2);
   ENSURE(B_MDUL, s * 4, S.MDUL);
+  ENSURE(B_SM, s * 8, S.SM);
+  ENSURE(B_SME, s * 8, S.SME);
   ENSURE(B_STATUS, 4, S.status);
   cudaStream_t st = ctx->stream;
   CUDA_OK(cudaMemsetAsync(S.status, 0, 4, st));
@@ -168,6 +214,7 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   CUDA_OK(cudaMemcpyAsync(&status, S.status, 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));
   if (status & 1) return DTWJ_ERR_NAN;
+  if (ph) ph->begin();
   launch_prep(S, st);
   if (masked) {
     const int lt_max = mask_table_max(m);
@@ -184,6 +231,7 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
     CUDA_OK(cudaMemsetAsync(S.mask, 0, n * 4, st));
   }
   launch_rowterms(S, masked, st);
+  if (ph) ph->end(DTWJ_PHASE_PREP, masked ? 9 : 4);
   CUDA_OK(cudaGetLastError());
   *out = S;
   return DTWJ_OK;
@@ -201,10 +249,11 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   const bool masked = !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
   const bool verbose = flags & DTWJ_F_VERBOSE;
   cudaStream_t st = ctx->stream;
+  Phases ph(ctx, (flags & DTWJ_F_PROFILE) != 0);
   CUDA_OK(cudaEventRecord(ctx->ev0, st));
 
   DevSeries S;
-  int rc = prepare(ctx, x_dev, n, m, w, masked, &S);
+  int rc = prepare(ctx, x_dev, n, m, w, masked, &S, &ph);
   if (rc) return rc;
   const int64_t s = S.s;
 
@@ -240,31 +289,28 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
 
   // ---- ED profile seeds ----
   float seed_bsf2 = INFINITY;
+  unsigned int* seed_slot = nullptr;
   if (!(flags & DTWJ_F_NO_SEED)) {
     unsigned long long* keys;
     ENSURE(B_KEYS_UP, s * 8, keys);
+    ph.begin();
     launch_mp(S, tiles, ntiles, keys, false, st);
+    ph.end(DTWJ_PHASE_PROFILE, 2);
     int2* seeds;
     unsigned int* nseeds;
     ENSURE(B_SEEDS, kSeeds * sizeof(int2), seeds);
     ENSURE(B_NSEEDS, 16, nseeds);
     CUDA_OK(cudaMemsetAsync(nseeds, 0, 16, st));
+    ph.begin();
     launch_seed_select(S, keys, seeds, nseeds, Q.bsf2, st);
     CUDA_OK(cudaMemsetAsync(nseeds + 1, 0, 4, st));
     DevSearch Qs = Q;
     Qs.queue_next = nseeds + 1;
     Qs.queue_cap = kSeeds;
-    launch_pairs(S, Qs, seeds, nseeds, masked, false, band, ctx->num_sms, st);
-    unsigned int b2 = 0;
-    CUDA_OK(cudaMemcpyAsync(&b2, Q.bsf2, 4, cudaMemcpyDeviceToHost, st));
-    if (verbose) {
-      CUDA_OK(cudaStreamSynchronize(st));
-      memcpy(&seed_bsf2, &b2, 4);
-      fprintf(stderr, "dtwj: seeds done, bsf %.6f, %.3fs\n", std::sqrt(seed_bsf2), wall.seconds());
-    } else {
-      CUDA_OK(cudaStreamSynchronize(st));
-      memcpy(&seed_bsf2, &b2, 4);
-    }
+    launch_pairs(S, Qs, seeds, nseeds, false, band, ctx->num_sms, st);
+    ph.end(DTWJ_PHASE_SEEDS, 2);
+    CUDA_OK(cudaMemcpyAsync(nseeds + 2, Q.bsf2, 4, cudaMemcpyDeviceToDevice, st));
+    seed_slot = nseeds + 2;
   }
 
   // ---- diagonal sweep in chunks ----
@@ -273,8 +319,12 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   for (int t0 = 0; t0 < ntiles; t0 += chunk) {
     const int t1 = t0 + chunk < ntiles ? t0 + chunk : ntiles;
     CUDA_OK(cudaMemsetAsync(qc, 0, 8, st));
-    launch_lb(S, Q, tiles, t0, t1, enumerate_all, st);
-    launch_pairs(S, Q, Q.queue, Q.queue_count, masked, !enumerate_all, band, ctx->num_sms, st);
+    ph.begin();
+    launch_lb(S, Q, tiles, t0, t1, masked, enumerate_all, st);
+    ph.end(DTWJ_PHASE_DIAG, 1);
+    ph.begin();
+    launch_pairs(S, Q, Q.queue, Q.queue_count, true, band, ctx->num_sms, st);
+    ph.end(DTWJ_PHASE_PAIRS, 1);
   }
   CUDA_OK(cudaGetLastError());
 
@@ -284,7 +334,9 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   double* best;
   ENSURE(B_BEST, 16, best);
   int* best_idx = reinterpret_cast<int*>(best + 1);
+  ph.begin();
   launch_verify(S, Q, band, vd2, best, best_idx, st);
+  ph.end(DTWJ_PHASE_VERIFY, 2);
   CUDA_OK(cudaEventRecord(ctx->ev1, st));
 
   double best_h[2];
@@ -296,6 +348,7 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   CUDA_OK(cudaMemcpyAsync(&cand_h, Q.cand_count, 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaMemcpyAsync(&bsf_h, Q.bsf2, 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaMemcpyAsync(&status_h, S.status, 4, cudaMemcpyDeviceToHost, st));
+  if (seed_slot) CUDA_OK(cudaMemcpyAsync(&seed_bsf2, seed_slot, 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));
   if (status_h & 2) return DTWJ_ERR_OVERFLOW;
   if (cand_h > kCandCap) return DTWJ_ERR_OVERFLOW;
@@ -334,6 +387,7 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   out->candidates = cand_h;
   out->seconds_join = ms / 1000.0;
   out->seconds_total = wall.seconds() + t_upload;
+  ph.collect(out);
   (void)bsf_h;
   if (verbose)
     fprintf(stderr, "dtwj: join (%lld, %lld) %.6f, %.3fs device\n", (long long)out->i,
@@ -388,6 +442,7 @@ void dtwj_ctx_destroy(dtwj_ctx* c) {
   cudaStreamSynchronize(c->stream);
   for (auto& b : c->bufs)
     if (b.p) cudaFree(b.p);
+  for (auto e : c->pool) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);

@@ -1,10 +1,9 @@
-// Per-pair stages: endpoint bound, masked diagonal bound, LB_Keogh in both
-// directions with its cumulative bound, and the banded DTW itself.
+// Per-pair stages for the survivors of the diagonal sweep: endpoint bound,
+// LB_Keogh in both directions with its cumulative bound, and the banded DTW.
 //
 // Reference counterparts:
 //   endpoint bound  LB_KIM / the tail of diag_mask_global
 //                   CPU_version1/lb_kim.cpp:10-73, GPU_version1/lib/diag_mask_global.cu:165-228
-//   masked bound    diag_mask_global  CPU_version1/diag_mask_global.cpp:11-226
 //   LB_Keogh        LB_KK             CPU_version1/lb_keogh.cpp:9-72,
 //                   lb_keogh_stride_with_nomalise  GPU_version1/src/LB_keogh_warp.cu:74-96
 //   DTW             MON_dtw           CPU_version1/MON_DTW.cpp:20-108,
@@ -181,32 +180,6 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
   return result;
 }
 
-// Endpoint bound: minimum cost of any warping path's cells in the first and
-// last three layers (LB_KIM, CPU_version1/lb_kim.cpp:10-73).  q = window i,
-// t = window j; the reference's fourth option adds the corner twice
-// (lb_kim.cpp:55,62), here it is added once so the bound stays admissible.
-__device__ void kim_bound(const float* q, const float* t, int m, float* left, float* right) {
-#define D2(x, y) (((x) - (y)) * ((x) - (y)))
-  const float o = D2(t[0], q[0]);
-  const float lw = fminf(D2(t[1], q[0]), D2(t[1], q[1]));
-  const float l1 = fminf(lw, D2(t[0], q[1]));
-  float d = fminf(D2(t[1], q[0]) + D2(t[2], q[0]), lw + D2(t[2], q[1]));
-  d = fminf(d, D2(q[1], t[1]) + D2(q[2], t[2]));
-  d = fminf(d, l1 + D2(q[2], t[1]));
-  d = fminf(d, D2(q[1], t[0]) + D2(q[2], t[0]));
-  *left = o + d;
-  const int e = m - 1;
-  const float o2 = D2(t[e], q[e]);
-  const float rw = fminf(D2(t[e - 1], q[e]), D2(t[e - 1], q[e - 1]));
-  const float r1 = fminf(rw, D2(t[e], q[e - 1]));
-  d = fminf(D2(t[e - 1], q[e]) + D2(t[e - 2], q[e]), rw + D2(t[e - 2], q[e - 1]));
-  d = fminf(d, D2(q[e - 1], t[e - 1]) + D2(q[e - 2], t[e - 2]));
-  d = fminf(d, r1 + D2(q[e - 2], t[e - 1]));
-  d = fminf(d, D2(q[e - 1], t[e]) + D2(q[e - 2], t[e]));
-  *right = o2 + d;
-#undef D2
-}
-
 // Envelope of z-normalised window `sub` (subs_U / subs_L of the reference) at
 // offset k: raw envelope in the interior, prefix / suffix extremes of the
 // window near its ends (the clipped window of lower_upper_lemire).
@@ -239,8 +212,7 @@ __device__ __forceinline__ float keogh_term(float x, float U, float L) {
 }
 
 // The pair consumer: every group takes pairs from the queue until it is
-// drained.  flags bit 0: run the bounds (otherwise DTW only, for seeds);
-// bit 1: run the masked bound.
+// drained.  flags bit 0: run the bounds (otherwise DTW only, for seeds).
 template <int C, int G>
 __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const int2* pairs,
                                                 const unsigned int* npairs, int flags,
@@ -248,7 +220,7 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
   extern __shared__ __align__(16) unsigned char smraw[];
   float* sm = reinterpret_cast<float*>(smraw);
   __shared__ unsigned long long cnt[kNumCounters];
-  const bool bounds = flags & 1, masked = flags & 2;
+  const bool bounds = flags & 1;
   const int m = S.m, w = S.w;
   const int gib = threadIdx.x / G, g = threadIdx.x % G;
   const unsigned int gm = group_mask<G>();
@@ -279,16 +251,28 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
     const int64_t i = pr.x, j = pr.y;
     const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
     float thr = __uint_as_float(*(volatile unsigned int*)Q.bsf2) * (1.0f + kSlack);
-    for (int k = g; k < m; k += G) {
-      q[k] = (float)((S.a[i + k] - mi) * si);
-      t[k] = (float)((S.a[j + k] - mj) * sj);
-    }
     for (int x = g; x <= lay.nc + 1; x += G) cbc[x] = 0.0f;
-    __syncwarp(gm);
-    if (bounds) {
-      // ---- endpoint bound ----
+    if (!bounds) {
+      for (int k = g; k < m; k += G) {
+        q[k] = (float)((S.a[i + k] - mi) * si);
+        t[k] = (float)((S.a[j + k] - mj) * sj);
+      }
+      __syncwarp(gm);
+    } else {
+      // ---- window ends first: endpoint bound and clipped edge envelopes ----
+      const int e2 = lay.e2;
+      const int tail = m - e2 > e2 ? m - e2 : e2;  // first position of the tail region
+      for (int k = g; k < e2; k += G) {
+        q[k] = (float)((S.a[i + k] - mi) * si);
+        t[k] = (float)((S.a[j + k] - mj) * sj);
+      }
+      for (int k = tail + g; k < m; k += G) {
+        q[k] = (float)((S.a[i + k] - mi) * si);
+        t[k] = (float)((S.a[j + k] - mj) * sj);
+      }
+      __syncwarp(gm);
       float kl = 0.0f, kr = 0.0f;
-      if (g == 0) kim_bound(q, t, m, &kl, &kr);
+      if (g == 0) kim_bound<float>(q, t, m, &kl, &kr);
       kl = __shfl_sync(gm, kl, 0, G);
       kr = __shfl_sync(gm, kr, 0, G);
       if (kl + kr > thr) {
@@ -296,81 +280,67 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
         __syncwarp(gm);
         continue;
       }
-      // ---- masked diagonal bound (diag_mask_global) ----
-      if (masked) {
-        float s1 = 0, s2 = 0, r1 = 0, r2 = 0;
-        for (int k = kBias + g; k <= m - 1 - kBias; k += G) {
-          const float Mi = S.mask[i + k], Mj = S.mask[j + k];
-          const float ei = (float)((S.E[i + k] - 2.0 * mi) * si);
-          const float ej = (float)((S.E[j + k] - 2.0 * mj) * sj);
-          const float qj = t[k], qi = q[k];
-          s1 = fmaf(Mi * qj, qj, s1);
-          s2 = fmaf(Mi * qj, ei, s2);
-          r1 = fmaf(Mj * qi, qi, r1);
-          r2 = fmaf(Mj * qi, ej, r2);
-        }
-        s1 = group_sum<G>(s1, gm);
-        s2 = group_sum<G>(s2, gm);
-        r1 = group_sum<G>(r1, gm);
-        r2 = group_sum<G>(r2, gm);
-        const float df = 2.0f * s1 - 2.0f * s2 + S.MN[i];
-        const float dr = 2.0f * r1 - 2.0f * r2 + S.MN[j];
-        const float lf = df < S.MDUL2[i] ? 0.0f : 0.5f * (sqrtf(2.0f * df - S.MDUL2[i]) - S.MDUL[i]);
-        const float lr = dr < S.MDUL2[j] ? 0.0f : 0.5f * (sqrtf(2.0f * dr - S.MDUL2[j]) - S.MDUL[j]);
-        const float lbm = fmaxf(lf, lr);
-        if (lbm > 0.0f && lbm * lbm > thr) {
-          if (g == 0) atomicAdd(&cnt[kPrunedMasked], 1ull);
-          __syncwarp(gm);
-          continue;
-        }
-        if (kl + kr + lbm * lbm > thr) {
-          if (g == 0) atomicAdd(&cnt[kPrunedKim], 1ull);
-          __syncwarp(gm);
-          continue;
-        }
-      }
-      // ---- clipped envelopes near the window ends ----
-      {
-        const int e2 = lay.e2;
-        for (int sc = g; sc < 8; sc += G) {
-          const float* z = (sc >> 2) ? t : q;
-          float* out = edge + sc * e2;
-          const int kind = sc & 3;
-          if (kind < 2) {
-            float acc = z[0];
-            for (int p = 0; p < e2; ++p) {
-              acc = kind == 0 ? fmaxf(acc, z[p]) : fminf(acc, z[p]);
-              out[p] = acc;
-            }
-          } else {
-            float acc = z[m - 1];
-            for (int p = m - 1; p >= m - e2; --p) {
-              acc = kind == 2 ? fmaxf(acc, z[p]) : fminf(acc, z[p]);
-              out[p - (m - e2)] = acc;
-            }
+      for (int sc = g; sc < 8; sc += G) {
+        const float* z = (sc >> 2) ? t : q;
+        float* out = edge + sc * e2;
+        const int kind = sc & 3;
+        if (kind < 2) {
+          float acc = z[0];
+          for (int p = 0; p < e2; ++p) {
+            acc = kind == 0 ? fmaxf(acc, z[p]) : fminf(acc, z[p]);
+            out[p] = acc;
+          }
+        } else {
+          float acc = z[m - 1];
+          for (int p = m - 1; p >= m - e2; --p) {
+            acc = kind == 2 ? fmaxf(acc, z[p]) : fminf(acc, z[p]);
+            out[p - (m - e2)] = acc;
           }
         }
       }
       __syncwarp(gm);
       // edge layout: [0..3] window i: pu, pl, su, sl; [4..7] window j
-      const EdgeEnv Ei = {edge, edge + lay.e2, edge + 2 * lay.e2, edge + 3 * lay.e2, lay.e2};
-      const EdgeEnv Ej = {edge + 4 * lay.e2, edge + 5 * lay.e2, edge + 6 * lay.e2,
-                          edge + 7 * lay.e2, lay.e2};
-      // ---- LB_Keogh both directions (LB_KK, lb_keogh.cpp:9-72) ----
+      const EdgeEnv Ei = {edge, edge + e2, edge + 2 * e2, edge + 3 * e2, e2};
+      const EdgeEnv Ej = {edge + 4 * e2, edge + 5 * e2, edge + 6 * e2, edge + 7 * e2, e2};
+      // ---- LB_Keogh both directions (LB_KK, lb_keogh.cpp:9-72), in rounds of
+      // 8G positions with early abandoning; the middle of both windows is
+      // z-normalised into shared memory on the way ----
       float e1 = 0, m1 = 0, e2s = 0, m2 = 0;
-      for (int k = g; k < m; k += G) {
-        float U, Lw;
-        envelope_at(S, j, mj, sj, Ej, k, &U, &Lw);
-        const float a1 = keogh_term(q[k], U, Lw);
-        envelope_at(S, i, mi, si, Ei, k, &U, &Lw);
-        const float a2 = keogh_term(t[k], U, Lw);
-        if (k < kBias || k >= m - kBias) {
-          e1 += a1;
-          e2s += a2;
-        } else {
-          m1 += a1;
-          m2 += a2;
+      bool dead = false;
+      for (int base = 0; base < m && !dead; base += 8 * G) {
+        const int lim = base + 8 * G < m ? base + 8 * G : m;
+        for (int k = base + g; k < lim; k += G) {
+          float qk, tk;
+          if (k >= e2 && k < tail) {
+            qk = (float)((S.a[i + k] - mi) * si);
+            tk = (float)((S.a[j + k] - mj) * sj);
+            q[k] = qk;
+            t[k] = tk;
+          } else {
+            qk = q[k];
+            tk = t[k];
+          }
+          float U, Lw;
+          envelope_at(S, j, mj, sj, Ej, k, &U, &Lw);
+          const float a1 = keogh_term(qk, U, Lw);
+          envelope_at(S, i, mi, si, Ei, k, &U, &Lw);
+          const float a2 = keogh_term(tk, U, Lw);
+          if (k < kBias || k >= m - kBias) {
+            e1 += a1;
+            e2s += a2;
+          } else {
+            m1 += a1;
+            m2 += a2;
+          }
         }
+        const float p1 = fmaxf(group_sum<G>(e1, gm), kl + kr) + group_sum<G>(m1, gm);
+        const float p2 = fmaxf(group_sum<G>(e2s, gm), kl + kr) + group_sum<G>(m2, gm);
+        if (p1 > thr || p2 > thr) dead = true;
+      }
+      if (dead) {
+        if (g == 0) atomicAdd(&cnt[kPrunedKeogh], 1ull);
+        __syncwarp(gm);
+        continue;
       }
       e1 = group_sum<G>(e1, gm);
       m1 = group_sum<G>(m1, gm);
@@ -378,11 +348,7 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
       m2 = group_sum<G>(m2, gm);
       const float lb1 = fmaxf(e1, kl + kr) + m1;
       const float lb2 = fmaxf(e2s, kl + kr) + m2;
-      if (lb1 > thr || lb2 > thr) {
-        if (g == 0) atomicAdd(&cnt[kPrunedKeogh], 1ull);
-        __syncwarp(gm);
-        continue;
-      }
+      __syncwarp(gm);
       // ---- cumulative bound of the larger direction, 8-cell chunks ----
       const bool dir1 = lb1 > lb2;
       for (int x = g; x < lay.nc; x += G) {
@@ -667,9 +633,9 @@ bool choose_band(int w, BandShape* out) {
 }
 
 void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
-                  const unsigned int* npairs, bool masked, bool bounds, BandShape band,
-                  int num_sms, cudaStream_t st) {
-  const int flags = (bounds ? 1 : 0) | (masked ? 2 : 0);
+                  const unsigned int* npairs, bool bounds, BandShape band, int num_sms,
+                  cudaStream_t st) {
+  const int flags = bounds ? 1 : 0;
 #define X(c, g) \
   if (band.C == c && band.G == g) { run_pairs<c, g>(S, Q, pairs, npairs, flags, num_sms, st); return; }
   DTWJ_BAND_CASES(X)

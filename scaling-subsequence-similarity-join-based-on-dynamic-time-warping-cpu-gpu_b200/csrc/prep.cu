@@ -85,7 +85,7 @@ __global__ void k_rowterms(DevSeries S, bool masked) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= S.s) return;
   const double mu = S.mu[i], isg = S.isg[i];
-  double N = 0, D2 = 0, sE = 0, MN = 0, MD2 = 0;
+  double N = 0, D2 = 0, sE = 0, MN = 0, MD2 = 0, SM = 0, SME = 0;
   const int m = S.m;
   for (int k = 0; k < m; ++k) {
     const double U = S.U[i + k], L = S.L[i + k];
@@ -95,7 +95,11 @@ __global__ void k_rowterms(DevSeries S, bool masked) {
     D2 = fma(u - l, u - l, D2);
     if (masked) {
       const double M = S.mask[i + k];
-      if (k >= kBias && k <= m - 1 - kBias) MN += M * (u * u + l * l);
+      if (k >= kBias && k <= m - 1 - kBias) {
+        MN += M * (u * u + l * l);
+        SM += M;
+        SME += M * (U + L);
+      }
       MD2 += M * (u - l) * (u - l);
     }
   }
@@ -113,6 +117,8 @@ __global__ void k_rowterms(DevSeries S, bool masked) {
     S.MN[i] = (float)MN;
     S.MDUL2[i] = (float)MD2;
     S.MDUL[i] = (float)sqrt(fmax(MD2, 0.0));
+    S.SM[i] = SM;
+    S.SME[i] = SME;
   }
 }
 
