@@ -62,9 +62,10 @@ extern "C" {
 #define DTWJ_PHASE_PROFILE 1    /* ED matrix profile                          */
 #define DTWJ_PHASE_SEEDS 2      /* seed selection and seed DTWs               */
 #define DTWJ_PHASE_DIAG 3       /* diagonal bound sweep                       */
-#define DTWJ_PHASE_PAIRS 4      /* endpoint / LB_Keogh / DTW on survivors     */
+#define DTWJ_PHASE_PAIRS 4      /* LB_Keogh with cumulative bound + DTW       */
 #define DTWJ_PHASE_VERIFY 5     /* FP64 re-verification                       */
-#define DTWJ_NUM_PHASES 6
+#define DTWJ_PHASE_RUNS 6       /* masked / endpoint / LB_Keogh on runs       */
+#define DTWJ_NUM_PHASES 7
 
 typedef struct {
   int64_t i, j;            /* top-1 pair, 0-based, j - i >= m                */

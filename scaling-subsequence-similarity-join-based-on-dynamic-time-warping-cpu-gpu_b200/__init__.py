@@ -41,7 +41,7 @@ F_LEARNED = 0x8
 F_VERBOSE = 0x10
 F_PROFILE = 0x20
 
-PHASES = ("prep", "profile", "seeds", "diag", "pairs", "verify")
+PHASES = ("prep", "profile", "seeds", "diag", "pairs", "verify", "runs")
 
 # Every symbol include/dtwj.h declares.
 EXPORTS = (

@@ -12,6 +12,19 @@ namespace dtwj {
 // below this; the slack keeps every pair whose true distance can still be the
 // minimum, and the final candidates are re-verified in FP64.
 constexpr float kSlack = 1.0f / 512.0f;
+// Absolute slack per window sample on squared distances: keeps a pair whose
+// distance ties the best-so-far (exact duplicates give 0) above the rounding
+// of the FP32 bounds.
+constexpr float kAbsSlackPerSample = 1e-6f;
+
+// Pruning / abandoning threshold on squared distances from the best-so-far.
+__device__ __forceinline__ float prune_threshold(unsigned int bsf2_bits, int m) {
+  return __uint_as_float(bsf2_bits) * (1.0f + kSlack) + kAbsSlackPerSample * (float)m;
+}
+__device__ __forceinline__ float prune_threshold_now(const unsigned int* bsf2, int m) {
+  return prune_threshold(*(volatile const unsigned int*)bsf2, m);
+}
+
 // Endpoint bound width (the reference's BIAS, CPU_version1/diag_mask_global.cpp:8).
 constexpr int kBias = 3;
 // Seeds taken from the ED matrix profile (CPU_version1/new_dtw_motifGUI.cpp:53).
@@ -33,6 +46,12 @@ struct Tile {
   int32_t order;  // position in the queue order (learned or plain)
 };
 constexpr int kTileLags = 128;
+// Longest run of consecutive surviving rows the sweep emits as one item.
+constexpr int kRunMax = 256;
+// FP32 copies of the series and its envelopes are centered per block of
+// 2^kBlkShift samples (value minus the block mean) so that the float rounding
+// error stays far below the pruning slack.
+constexpr int kBlkShift = 10;
 
 // Counters, all uint64 on the device.
 enum Counter {
@@ -81,6 +100,10 @@ struct DevSeries {
   float* MDUL;      // s
   double* SM;       // s, sum_T M            (T = [kBias, m-1-kBias])
   double* SME;      // s, sum_T M E
+  double* cb;       // (n >> kBlkShift) + 2, block centers
+  float* af;        // n, a - cb[block]
+  float* Uf;        // n, U - cb[block]
+  float* Lf;        // n, L - cb[block]
   int* status;      // device status word (0 ok, else error bits)
 };
 
@@ -91,6 +114,10 @@ struct DevSearch {
   Candidate* cand;              // candidate list
   unsigned int* cand_count;
   unsigned int cand_cap;
+  int4* runs;                   // runs of fast-bound survivors: (i0, j0, len, 0)
+  unsigned int* run_count;
+  unsigned int* run_next;
+  unsigned int run_cap;
   int2* queue;                  // survivor pairs of the current chunk
   unsigned int* queue_count;
   unsigned int* queue_next;
@@ -148,10 +175,15 @@ void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
                         cudaStream_t st);
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
                         unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st);
-// masked: evaluate the masked bound; enumerate_all: no pruning, every pair
-// goes to the queue (diagonal bounds disabled)
+// Fast diagonal bound over tiles [tile_begin, tile_end); survivors leave as
+// runs of consecutive rows.  enumerate_all: no pruning (diagonal bounds off).
 void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
-               int tile_end, bool masked, bool enumerate_all, cudaStream_t st);
+               int tile_end, bool enumerate_all, cudaStream_t st);
+// Run filter: masked bound, endpoint bound and LB_Keogh for every pair of
+// every run; pairs that survive go to Q.queue.
+void launch_runs(const DevSeries& S, const DevSearch& Q, bool masked, bool bounds, int num_sms,
+                 cudaStream_t st);
+void launch_center(const DevSeries& S, cudaStream_t st);
 // bounds = false: DTW only (the seeds); true: endpoint bound + LB_Keogh first
 void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
                   const unsigned int* npairs, bool bounds, BandShape band, int num_sms,

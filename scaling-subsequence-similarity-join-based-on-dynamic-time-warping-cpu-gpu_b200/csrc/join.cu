@@ -65,7 +65,7 @@ enum BufId {
   B_AC, B_DUL, B_QSIG, B_MASK, B_MN, B_MDUL2, B_MDUL, B_SM, B_SME, B_STATUS,
   B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_KEYS_LO, B_TILES, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
-  B_MP, B_MPI,
+  B_MP, B_MPI, B_CB, B_AF, B_UF, B_LF, B_RUNS,
   B_COUNT_
 };
 
@@ -206,6 +206,10 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   ENSURE(B_MDUL, s * 4, S.MDUL);
   ENSURE(B_SM, s * 8, S.SM);
   ENSURE(B_SME, s * 8, S.SME);
+  ENSURE(B_CB, ((n >> kBlkShift) + 4) * 8, S.cb);
+  ENSURE(B_AF, n * 4, S.af);
+  ENSURE(B_UF, n * 4, S.Uf);
+  ENSURE(B_LF, n * 4, S.Lf);
   ENSURE(B_STATUS, 4, S.status);
   cudaStream_t st = ctx->stream;
   CUDA_OK(cudaMemsetAsync(S.status, 0, 4, st));
@@ -231,7 +235,8 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
     CUDA_OK(cudaMemsetAsync(S.mask, 0, n * 4, st));
   }
   launch_rowterms(S, masked, st);
-  if (ph) ph->end(DTWJ_PHASE_PREP, masked ? 9 : 4);
+  launch_center(S, st);
+  if (ph) ph->end(DTWJ_PHASE_PREP, masked ? 11 : 6);
   CUDA_OK(cudaGetLastError());
   *out = S;
   return DTWJ_OK;
@@ -269,14 +274,22 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   memset(&Q, 0, sizeof Q);
   const double total_pairs = 0.5 * (double)(s - m) * (double)(s - m + 1);
   unsigned int qcap = kQueueCapMax;
+  if (const char* env = getenv("DTWJ_QUEUE_CAP")) {  // smaller chunks (profiling)
+    const long v = atol(env);
+    if (v >= (long)kTileLags * kTileRows && v < (long)kQueueCapMax) qcap = (unsigned int)v;
+  }
   if (total_pairs < (double)qcap) qcap = (unsigned int)total_pairs + 1024;
   const int tiles_per_chunk_max = (int)(qcap / ((unsigned)kTileLags * kTileRows));
   ENSURE(B_QUEUE, (size_t)qcap * sizeof(int2), Q.queue);
+  ENSURE(B_RUNS, (size_t)qcap * sizeof(int4), Q.runs);
   unsigned int* qc;
   ENSURE(B_QCOUNT, 16, qc);
   Q.queue_count = qc;
   Q.queue_next = qc + 1;
+  Q.run_count = qc + 2;
+  Q.run_next = qc + 3;
   Q.queue_cap = qcap;
+  Q.run_cap = qcap;
   ENSURE(B_BSF2, 4, Q.bsf2);
   ENSURE(B_COUNTERS, kNumCounters * 8, Q.counters);
   ENSURE(B_CAND, (size_t)kCandCap * sizeof(Candidate), Q.cand);
@@ -318,10 +331,13 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   int chunk = tiles_per_chunk_max > 0 ? tiles_per_chunk_max : 1;
   for (int t0 = 0; t0 < ntiles; t0 += chunk) {
     const int t1 = t0 + chunk < ntiles ? t0 + chunk : ntiles;
-    CUDA_OK(cudaMemsetAsync(qc, 0, 8, st));
+    CUDA_OK(cudaMemsetAsync(qc, 0, 16, st));
     ph.begin();
-    launch_lb(S, Q, tiles, t0, t1, masked, enumerate_all, st);
+    launch_lb(S, Q, tiles, t0, t1, enumerate_all, st);
     ph.end(DTWJ_PHASE_DIAG, 1);
+    ph.begin();
+    launch_runs(S, Q, masked, !enumerate_all, ctx->num_sms, st);
+    ph.end(DTWJ_PHASE_RUNS, 1);
     ph.begin();
     launch_pairs(S, Q, Q.queue, Q.queue_count, true, band, ctx->num_sms, st);
     ph.end(DTWJ_PHASE_PAIRS, 1);

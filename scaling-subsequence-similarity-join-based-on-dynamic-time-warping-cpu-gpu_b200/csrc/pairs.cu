@@ -153,7 +153,7 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
       int idx = r + w + 1;
       idx = idx < 0 ? 0 : (idx + 7) >> 3;
       const float cbv = cbc[idx < nc ? idx : nc];
-      const float fresh = __uint_as_float(*(volatile const unsigned int*)bsf2) * (1.0f + kSlack);
+      const float fresh = prune_threshold_now(bsf2, m);
       thr = fminf(thr, fresh);
       const bool over = (float)fm + cbv > thr;
       const unsigned int vote = __ballot_sync(gm, over);
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
     const int2 pr = pairs[idx];
     const int64_t i = pr.x, j = pr.y;
     const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
-    float thr = __uint_as_float(*(volatile unsigned int*)Q.bsf2) * (1.0f + kSlack);
+    float thr = prune_threshold_now(Q.bsf2, S.m);
     for (int x = g; x <= lay.nc + 1; x += G) cbc[x] = 0.0f;
     if (!bounds) {
       for (int k = g; k < m; k += G) {
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
       if (ab) {
         atomicAdd(&cnt[kDtwAbandoned], 1ull);
       } else {
-        const float now = __uint_as_float(*(volatile unsigned int*)Q.bsf2) * (1.0f + kSlack);
+        const float now = prune_threshold_now(Q.bsf2, S.m);
         if (d2 <= now) {
           atomicMin(Q.bsf2, __float_as_uint(d2));
           const unsigned int slot = atomicAdd(Q.cand_count, 1u);
@@ -449,7 +449,7 @@ __global__ void __launch_bounds__(128) k_dtw_list(DevSeries S, const int2* pairs
     const unsigned int c = *count_ptr;
     n = (int)(c < (unsigned)count ? c : (unsigned)count);
   }
-  const float fin = bsf2 ? __uint_as_float(*bsf2) * (1.0f + kSlack) : 0.0f;
+  const float fin = bsf2 ? prune_threshold(*bsf2, S.m) : 0.0f;
   for (int k = blockIdx.x * groups + gib; k < n; k += gridDim.x * groups) {
     int64_t i, j;
     if (cands) {

@@ -101,6 +101,8 @@ def workload(name: str):
     """Named workloads: returns dict(series=..., m=..., w=..., ...)."""
     if name == "rw20k":  # plain method, CPU-runnable
         return dict(series=random_walk(20_000, 0), m=256, w=band(256, 0.01), ratio=0.01)
+    if name == "rw65k":  # small case of the at-scale workload
+        return dict(series=random_walk(65_536, 3), m=1024, w=band(1024, 0.05), ratio=0.05)
     if name == "rw1m_motif":  # plain GPU at scale
         x = random_walk(1_000_000, 1)
         planted = plant_motifs(x, 1, 1024, 1)
