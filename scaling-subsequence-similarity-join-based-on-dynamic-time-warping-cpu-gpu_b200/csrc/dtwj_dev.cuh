@@ -46,6 +46,13 @@ struct Tile {
   int32_t order;  // position in the queue order (learned or plain)
 };
 constexpr int kTileLags = 128;
+// Diagonal-sweep tiles: 128 threads x kLbPerThread lags x kLbRows rows, one
+// survivor bit per pair, kLbWords 32-row words per lag.
+constexpr int kLbThreads = 128;
+constexpr int kLbPerThread = 7;
+constexpr int kLbLags = kLbThreads * kLbPerThread;
+constexpr int kLbRows = 18 * kLbPerThread * 32;
+constexpr int kLbWords = kLbRows / 32;
 // Longest run of consecutive surviving rows the sweep emits as one item.
 constexpr int kRunMax = 256;
 // FP32 copies of the series and its envelopes are centered per block of
@@ -175,13 +182,16 @@ void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
                         cudaStream_t st);
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
                         unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st);
-// Fast diagonal bound over tiles [tile_begin, tile_end); survivors leave as
-// runs of consecutive rows.  enumerate_all: no pruning (diagonal bounds off).
+// Fast diagonal bound over LB tiles [tile_begin, tile_end); survivors leave
+// as bits, [tile][lag][word].  enumerate_all: no pruning (bounds off).
 void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
-               int tile_end, bool enumerate_all, cudaStream_t st);
-// Run filter: masked bound, endpoint bound and LB_Keogh for every pair of
-// every run; pairs that survive go to Q.queue.
-void launch_runs(const DevSeries& S, const DevSearch& Q, bool masked, bool bounds, int num_sms,
+               int tile_end, unsigned int* bits, bool enumerate_all, cudaStream_t st);
+size_t lb_smem_bytes();
+// Run filter over the survivor bits of LB tiles [tile_begin, tile_end):
+// masked bound, endpoint bound and LB_Keogh for every pair of every run of
+// consecutive survivors; pairs that survive go to Q.queue.
+void launch_runs(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
+                 int tile_end, const unsigned int* bits, bool masked, bool bounds, int num_sms,
                  cudaStream_t st);
 void launch_center(const DevSeries& S, cudaStream_t st);
 // bounds = false: DTW only (the seeds); true: endpoint bound + LB_Keogh first

@@ -31,7 +31,8 @@ namespace {
 
 constexpr int kTileRows = 4096;
 constexpr unsigned int kCandCap = 1u << 20;
-constexpr unsigned int kQueueCapMax = 1u << 27;
+constexpr unsigned int kQueueCapMax = 1u << 26;
+constexpr int kLbChunkTiles = 1024;
 
 struct Buf {
   void* p = nullptr;
@@ -53,8 +54,10 @@ struct dtwj_ctx {
   int num_sms = 0;
   std::vector<Buf> bufs;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  std::vector<Tile> tiles_host;
+  std::vector<Tile> tiles_host;      // 128-lag tiles of the ED profile
   int64_t tiles_n = -1, tiles_m = -1;
+  std::vector<Tile> lbtiles_host;    // kLbLags-lag tiles of the diagonal sweep
+  int64_t lbtiles_n = -1, lbtiles_m = -1;
   std::vector<cudaEvent_t> pool;  // events for per-phase device times
 };
 
@@ -65,7 +68,7 @@ enum BufId {
   B_AC, B_DUL, B_QSIG, B_MASK, B_MN, B_MDUL2, B_MDUL, B_SM, B_SME, B_STATUS,
   B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_KEYS_LO, B_TILES, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
-  B_MP, B_MPI, B_CB, B_AF, B_UF, B_LF, B_RUNS,
+  B_MP, B_MPI, B_CB, B_AF, B_UF, B_LF, B_BITS, B_LBTILES,
   B_COUNT_
 };
 
@@ -174,6 +177,26 @@ void build_tiles(dtwj_ctx* ctx, int64_t n, int m) {
   ctx->tiles_m = m;
 }
 
+void build_lb_tiles(dtwj_ctx* ctx, int64_t n, int m) {
+  if (ctx->lbtiles_n == n && ctx->lbtiles_m == m) return;
+  const int64_t s = n - m + 1;
+  ctx->lbtiles_host.clear();
+  int32_t order = 0;
+  for (int64_t L0 = m; L0 <= s - 1; L0 += kLbLags) {
+    const int64_t rows_total = s - L0;
+    for (int64_t i0 = 0; i0 < rows_total; i0 += kLbRows) {
+      Tile t;
+      t.L0 = (int32_t)L0;
+      t.i0 = (int32_t)i0;
+      t.rows = (int32_t)(rows_total - i0 < kLbRows ? rows_total - i0 : kLbRows);
+      t.order = order++;
+      ctx->lbtiles_host.push_back(t);
+    }
+  }
+  ctx->lbtiles_n = n;
+  ctx->lbtiles_m = m;
+}
+
 // Allocates and prepares every per-series array; returns the DevSeries.
 int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool masked,
             DevSeries* out, Phases* ph = nullptr) {
@@ -272,16 +295,12 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   // search state
   DevSearch Q;
   memset(&Q, 0, sizeof Q);
-  const double total_pairs = 0.5 * (double)(s - m) * (double)(s - m + 1);
   unsigned int qcap = kQueueCapMax;
-  if (const char* env = getenv("DTWJ_QUEUE_CAP")) {  // smaller chunks (profiling)
+  if (const char* env = getenv("DTWJ_QUEUE_CAP")) {  // smaller queue (profiling, tests)
     const long v = atol(env);
-    if (v >= (long)kTileLags * kTileRows && v < (long)kQueueCapMax) qcap = (unsigned int)v;
+    if (v >= 1024 && v < (long)kQueueCapMax) qcap = (unsigned int)v;
   }
-  if (total_pairs < (double)qcap) qcap = (unsigned int)total_pairs + 1024;
-  const int tiles_per_chunk_max = (int)(qcap / ((unsigned)kTileLags * kTileRows));
   ENSURE(B_QUEUE, (size_t)qcap * sizeof(int2), Q.queue);
-  ENSURE(B_RUNS, (size_t)qcap * sizeof(int4), Q.runs);
   unsigned int* qc;
   ENSURE(B_QCOUNT, 16, qc);
   Q.queue_count = qc;
@@ -289,7 +308,8 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   Q.run_count = qc + 2;
   Q.run_next = qc + 3;
   Q.queue_cap = qcap;
-  Q.run_cap = qcap;
+  Q.runs = nullptr;
+  Q.run_cap = 0;
   ENSURE(B_BSF2, 4, Q.bsf2);
   ENSURE(B_COUNTERS, kNumCounters * 8, Q.counters);
   ENSURE(B_CAND, (size_t)kCandCap * sizeof(Candidate), Q.cand);
@@ -326,23 +346,44 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
     seed_slot = nseeds + 2;
   }
 
-  // ---- diagonal sweep in chunks ----
+  // ---- diagonal sweep in chunks of LB tiles ----
+  build_lb_tiles(ctx, n, m);
+  const int nlb = (int)ctx->lbtiles_host.size();
+  Tile* lbtiles;
+  ENSURE(B_LBTILES, (size_t)nlb * sizeof(Tile), lbtiles);
+  CUDA_OK(cudaMemcpyAsync(lbtiles, ctx->lbtiles_host.data(), (size_t)nlb * sizeof(Tile),
+                          cudaMemcpyHostToDevice, st));
   const bool enumerate_all = flags & DTWJ_F_NO_DIAG;
-  int chunk = tiles_per_chunk_max > 0 ? tiles_per_chunk_max : 1;
-  for (int t0 = 0; t0 < ntiles; t0 += chunk) {
-    const int t1 = t0 + chunk < ntiles ? t0 + chunk : ntiles;
-    CUDA_OK(cudaMemsetAsync(qc, 0, 16, st));
-    ph.begin();
-    launch_lb(S, Q, tiles, t0, t1, enumerate_all, st);
-    ph.end(DTWJ_PHASE_DIAG, 1);
-    ph.begin();
-    launch_runs(S, Q, masked, !enumerate_all, ctx->num_sms, st);
-    ph.end(DTWJ_PHASE_RUNS, 1);
-    ph.begin();
-    launch_pairs(S, Q, Q.queue, Q.queue_count, true, band, ctx->num_sms, st);
-    ph.end(DTWJ_PHASE_PAIRS, 1);
+  const double tile_pairs = (double)kLbLags * kLbRows;
+  int chunk = kLbChunkTiles;
+  if (enumerate_all) chunk = (int)((double)qcap / tile_pairs) > 0 ? (int)((double)qcap / tile_pairs) : 1;
+  unsigned int* bits;
+  ENSURE(B_BITS, (size_t)(chunk < nlb ? chunk : nlb) * kLbLags * kLbWords * 4, bits);
+  for (int attempt = 0;; ++attempt) {
+    for (int t0 = 0; t0 < nlb; t0 += chunk) {
+      const int t1 = t0 + chunk < nlb ? t0 + chunk : nlb;
+      CUDA_OK(cudaMemsetAsync(qc, 0, 16, st));
+      ph.begin();
+      launch_lb(S, Q, lbtiles, t0, t1, bits, enumerate_all, st);
+      ph.end(DTWJ_PHASE_DIAG, 1);
+      ph.begin();
+      launch_runs(S, Q, lbtiles, t0, t1, bits, masked, !enumerate_all, ctx->num_sms, st);
+      ph.end(DTWJ_PHASE_RUNS, 1);
+      ph.begin();
+      launch_pairs(S, Q, Q.queue, Q.queue_count, true, band, ctx->num_sms, st);
+      ph.end(DTWJ_PHASE_PAIRS, 1);
+    }
+    CUDA_OK(cudaGetLastError());
+    // a survivor queue that overflowed loses pairs: sweep again in smaller chunks
+    int sweep_status = 0;
+    CUDA_OK(cudaMemcpyAsync(&sweep_status, S.status, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    if (!(sweep_status & 2)) break;
+    if (chunk == 1 || attempt >= 4) return DTWJ_ERR_OVERFLOW;
+    chunk = chunk / 32 > 0 ? chunk / 32 : 1;
+    CUDA_OK(cudaMemsetAsync(S.status, 0, 4, st));
+    CUDA_OK(cudaMemsetAsync(Q.counters, 0, kNumCounters * 8, st));
   }
-  CUDA_OK(cudaGetLastError());
 
   // ---- FP64 verification of the candidates ----
   double* vd2;

@@ -1,7 +1,6 @@
 // Diagonal lower-bound sweep: the first stage of the reference's GLOBAL_DIAG
 // kernel (GPU_version1/lib/GLOBAL_DIAG.cu:29-73), diag_fast
-// (GPU_version1/lib/diag_fast.cu:13-90, CPU_version1/diag_fast.cpp:12-88),
-// for a tile of 128 lags x up to 4096 rows.
+// (GPU_version1/lib/diag_fast.cu:13-90, CPU_version1/diag_fast.cpp:12-88).
 //
 // For pair (i, j), j = i + L, and the raw-series envelope U, L (radius w)
 // normalised by window r, the reference bounds the z-normalised DTW by
@@ -11,120 +10,218 @@
 // along the diagonal in O(1).  lb > bsf  <=>  X < (A_r - (2 bsf + DUL_r)^2)/4
 // with A_r = 4m + 2N_r - DUL2_r, and X = C / (sig_q sig_r) with the centered
 // FP64 cross covariance C(r, q) = sum_k (a[q+k] - mu_q) (E[r+k] - nu_r),
-// E = U + L.  A direction therefore prunes iff  G_r sig_q - C > 0  with
+// E = U + L, which moves along a diagonal as
+//   C(r, q) = C(r-1, q-1) + df_a[q-1] dg_E[r-1] + df_E[r-1] dg_a[q-1].
+// A direction therefore prunes iff  G_r sig_q - C > 0  with
 // G_r = sig_r (A_r - (2 bsf + DUL_r)^2) / 4: two FP64 recurrences (4 DFMA)
 // and two DFMA tests per pair, no division and no square root.
 //
-// One thread owns one lag and walks the tile's rows; the block's 128 lags
-// share each row, so row operands are broadcast and column operands are
-// consecutive.  Survivors of one lag come in long runs of consecutive rows
-// (the bound moves slowly along a diagonal), so a thread emits
-// (i0, j0, length) per run, capped at kRunMax rows, with one atomic per warp
-// and row; the run filter (runs.cu) then reuses each run's data across its
-// pairs.
+// Tile: 128 threads x kLbPerThread consecutive lags x kLbRows rows.  Rows are
+// processed in stages of kStage rows: the block stages the column operands
+// (df_a, dg_a, df_E, dg_E of index j-1, sig and G of j) for the stage's
+// kLbLags + kStage columns and the row operands for its rows in shared
+// memory, with G computed from the current best-so-far while staging.  Each
+// thread keeps a sliding window of its kLbPerThread columns in registers, so
+// every shared load feeds kLbPerThread pairs (kLbPerThread is odd, so the
+// strided FP64 reads are bank-conflict free).  Survivors are written as one
+// bit per pair, 32 rows per word, [tile][lag][word]; the run filter
+// (runs.cu) turns the bits back into runs of consecutive rows.
 #include "dtwj_dev.cuh"
 
 namespace dtwj {
 namespace {
 
-__global__ void __launch_bounds__(kTileLags) k_lb(DevSeries S, DevSearch Q, const Tile* tiles,
-                                                  bool enumerate_all) {
+constexpr int kStage = kLbPerThread * 32;          // rows per shared-memory stage
+constexpr int kCols = kLbLags + kStage;            // staged columns per stage
+static_assert(kLbRows % kStage == 0, "tile rows must be whole stages");
+
+struct LbShared {
+  double p1[kCols], p2[kCols], p3[kCols], p4[kCols], sg[kCols], g[kCols];
+  double r1[kStage], r2[kStage], r3[kStage], r4[kStage], rs[kStage], rg[kStage];
+};
+
+__device__ __forceinline__ double g_of(const DevSeries& S, int64_t x, double twoB) {
+  const double t = twoB + S.DUL[x];
+  return S.qsig[x] * fma(-t, t, S.A[x]);
+}
+
+__global__ void __launch_bounds__(kLbThreads, 2) k_lb(DevSeries S, DevSearch Q,
+                                                      const Tile* tiles, unsigned int* bits,
+                                                      bool enumerate_all) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  LbShared& sh = *reinterpret_cast<LbShared*>(smraw);
   const Tile T = tiles[blockIdx.x];
-  const int64_t L = (int64_t)T.L0 + threadIdx.x;
   const int64_t s = S.s;
   const int m = S.m;
-  const int64_t i_begin = T.i0;
-  const int64_t i_end = (int64_t)T.i0 + T.rows < s - L ? (int64_t)T.i0 + T.rows : s - L;
-  const bool any = L < s && i_begin < i_end;
-  const int lane = threadIdx.x & 31;
+  const int t = threadIdx.x, lane = t & 31;
+  const int64_t L0 = T.L0, i0 = T.i0;
+  const int64_t Lt = L0 + (int64_t)t * kLbPerThread;  // this thread's first lag
+  unsigned int* out = bits + (size_t)blockIdx.x * kLbLags * kLbWords;
 
-  const float b2 = prune_threshold_now(Q.bsf2, S.m);
+  const float b2 = enumerate_all ? __int_as_float(0x7f800000) : prune_threshold_now(Q.bsf2, m);
   const double twoB = 2.0 * sqrt((double)b2);
 
-  double Cf = 0.0, Cr = 0.0;
-  if (any) {
-    const int64_t i = i_begin, j = i_begin + L;
-    const double mi = S.mu[i], mj = S.mu[j], ni = S.nu[i], nj = S.nu[j];
+  // ---- exact anchors at the tile's first row ----
+  double Cf[kLbPerThread], Cr[kLbPerThread];
+#pragma unroll
+  for (int l = 0; l < kLbPerThread; ++l) Cf[l] = Cr[l] = 0.0;
+  {
+    double mj[kLbPerThread], nj[kLbPerThread];
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) {
+      const int64_t j = i0 + Lt + l < s ? i0 + Lt + l : s - 1;
+      mj[l] = S.mu[j];
+      nj[l] = S.nu[j];
+    }
+    const double mi = S.mu[i0], ni = S.nu[i0];
+    const int64_t jb = i0 + Lt;
+    // sliding windows of a and E over the thread's columns
+    double wa[kLbPerThread], we[kLbPerThread];
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) {
+      const int64_t x = jb + l < S.n ? jb + l : S.n - 1;
+      wa[l] = S.a[x];
+      we[l] = S.E[x];
+    }
     for (int k = 0; k < m; ++k) {
-      Cf = fma(S.a[j + k] - mj, S.E[i + k] - ni, Cf);
-      Cr = fma(S.a[i + k] - mi, S.E[j + k] - nj, Cr);
+      const double ei = S.E[i0 + k] - ni, ai = S.a[i0 + k] - mi;
+#pragma unroll
+      for (int l = 0; l < kLbPerThread; ++l) {
+        Cf[l] = fma(wa[l] - mj[l], ei, Cf[l]);
+        Cr[l] = fma(ai, we[l] - nj[l], Cr[l]);
+      }
+#pragma unroll
+      for (int l = 0; l < kLbPerThread - 1; ++l) {
+        wa[l] = wa[l + 1];
+        we[l] = we[l + 1];
+      }
+      const int64_t x = jb + kLbPerThread + k < S.n ? jb + kLbPerThread + k : S.n - 1;
+      wa[kLbPerThread - 1] = S.a[x];
+      we[kLbPerThread - 1] = S.E[x];
     }
   }
-  unsigned long long npairs = 0, nfast = 0;
-  int64_t run_start = -1;
-  int run_len = 0;
-  for (int x = 0; x <= T.rows; ++x) {
-    const int64_t i = i_begin + x;
-    bool survive = false;
-    if (x < T.rows && any && i < i_end) {
-      const int64_t j = i + L;
-      if (x > 0) {
-        Cf = fma(S.dfa[j - 1], S.dgE[i - 1], Cf);
-        Cf = fma(S.dfE[i - 1], S.dga[j - 1], Cf);
-        Cr = fma(S.dfa[i - 1], S.dgE[j - 1], Cr);
-        Cr = fma(S.dfE[j - 1], S.dga[i - 1], Cr);
+
+  unsigned int npairs = 0, nfast = 0;
+  double w1[kLbPerThread], w2[kLbPerThread], w3[kLbPerThread], w4[kLbPerThread];
+  double ws[kLbPerThread], wg[kLbPerThread];
+  for (int st = 0; st < T.rows; st += kStage) {
+    const int64_t r0 = i0 + st;         // first row of the stage
+    const int64_t c0 = r0 + L0;         // first staged column
+    __syncthreads();
+    for (int x = t; x < kCols; x += kLbThreads) {
+      const int64_t j = c0 + x;
+      if (j >= 1 && j < s) {
+        sh.p1[x] = S.dfa[j - 1];
+        sh.p2[x] = S.dga[j - 1];
+        sh.p3[x] = S.dfE[j - 1];
+        sh.p4[x] = S.dgE[j - 1];
+        sh.sg[x] = S.sig[j];
+        sh.g[x] = g_of(S, j, twoB);
+      } else {
+        sh.p1[x] = sh.p2[x] = sh.p3[x] = sh.p4[x] = 0.0;
+        sh.sg[x] = 1.0;
+        sh.g[x] = 1e300;
       }
-      const double ti = twoB + S.DUL[i];
-      const double Gi = S.qsig[i] * fma(-ti, ti, S.A[i]);
-      const double tj = twoB + S.DUL[j];
-      const double Gj = S.qsig[j] * fma(-tj, tj, S.A[j]);
-      const bool prune = !enumerate_all &&
-                         (fma(Gi, S.sig[j], -Cf) > 0.0 || fma(Gj, S.sig[i], -Cr) > 0.0);
-      ++npairs;
-      if (prune) ++nfast;
-      else survive = true;
     }
-    // run bookkeeping: close a run when it breaks, hits kRunMax or the tile ends
-    bool emit = false;
-    int64_t e_start = 0;
-    int e_len = 0;
-    if (survive) {
-      if (run_start < 0) {
-        run_start = i;
-        run_len = 0;
+    for (int x = t; x < kStage; x += kLbThreads) {
+      const int64_t i = r0 + x;
+      if (i >= 1 && i < s) {
+        sh.r1[x] = S.dfa[i - 1];
+        sh.r2[x] = S.dga[i - 1];
+        sh.r3[x] = S.dfE[i - 1];
+        sh.r4[x] = S.dgE[i - 1];
+        sh.rs[x] = S.sig[i];
+        sh.rg[x] = g_of(S, i, twoB);
+      } else {
+        sh.r1[x] = sh.r2[x] = sh.r3[x] = sh.r4[x] = 0.0;
+        sh.rs[x] = 1.0;
+        sh.rg[x] = 1e300;
       }
-      ++run_len;
-      if (run_len == kRunMax) {
-        emit = true;
-        e_start = run_start;
-        e_len = run_len;
-        run_start = -1;
-      }
-    } else if (run_start >= 0) {
-      emit = true;
-      e_start = run_start;
-      e_len = run_len;
-      run_start = -1;
     }
-    const unsigned int ballot = __ballot_sync(0xffffffffu, emit);
-    if (ballot) {
-      const int leader = __ffs(ballot) - 1;
-      unsigned int base = 0;
-      if (lane == leader) base = atomicAdd(Q.run_count, (unsigned int)__popc(ballot));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (emit) {
-        const unsigned int slot = base + __popc(ballot & ((1u << lane) - 1u));
-        if (slot < Q.run_cap) Q.runs[slot] = make_int4((int)e_start, (int)(e_start + L), e_len, 0);
-        else atomicOr(S.status, 2);
+    __syncthreads();
+    // windows: column of lag l at stage row 0 is stage column t*K + l
+    const int cb = t * kLbPerThread;
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) {
+      w1[l] = sh.p1[cb + l];
+      w2[l] = sh.p2[cb + l];
+      w3[l] = sh.p3[cb + l];
+      w4[l] = sh.p4[cb + l];
+      ws[l] = sh.sg[cb + l];
+      wg[l] = sh.g[cb + l];
+    }
+    unsigned int word[kLbPerThread];
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) word[l] = 0u;
+    for (int qq = 0; qq < kStage / kLbPerThread; ++qq) {
+#pragma unroll
+      for (int u = 0; u < kLbPerThread; ++u) {
+        const int r = qq * kLbPerThread + u;   // stage row; r % K == u
+        const int64_t i = r0 + r;
+        const bool row_ok = st + r < T.rows;
+        const bool first = (st == 0 && r == 0);
+        const double q1 = sh.r1[r], q2 = sh.r2[r], q3 = sh.r3[r], q4 = sh.r4[r];
+        const double qs = sh.rs[r], qg = sh.rg[r];
+#pragma unroll
+        for (int l = 0; l < kLbPerThread; ++l) {
+          const int sl = (u + l) % kLbPerThread;  // ring slot of lag l at this row
+          if (!first) {
+            Cf[l] = fma(w1[sl], q4, Cf[l]);
+            Cf[l] = fma(q3, w2[sl], Cf[l]);
+            Cr[l] = fma(q1, w4[sl], Cr[l]);
+            Cr[l] = fma(w3[sl], q2, Cr[l]);
+          }
+          const bool valid = row_ok && i + Lt + l < s;
+          const bool prune = !enumerate_all &&
+                             (fma(qg, ws[sl], -Cf[l]) > 0.0 || fma(wg[sl], qs, -Cr[l]) > 0.0);
+          npairs += valid ? 1u : 0u;
+          nfast += (valid && prune) ? 1u : 0u;
+          word[l] |= (valid && !prune ? 1u : 0u) << (r & 31);
+        }
+        // the column lag K-1 needs at the next row replaces the one lag 0 used
+        const int nx = cb + r + kLbPerThread;
+        w1[u] = sh.p1[nx];
+        w2[u] = sh.p2[nx];
+        w3[u] = sh.p3[nx];
+        w4[u] = sh.p4[nx];
+        ws[u] = sh.sg[nx];
+        wg[u] = sh.g[nx];
+        if ((r & 31) == 31) {
+          const int wi = (st + r) >> 5;
+#pragma unroll
+          for (int l = 0; l < kLbPerThread; ++l) {
+            out[(size_t)(t * kLbPerThread + l) * kLbWords + wi] = word[l];
+            word[l] = 0u;
+          }
+        }
       }
     }
   }
+  unsigned long long np = npairs, nf = nfast;
   for (int o = 16; o > 0; o >>= 1) {
-    npairs += __shfl_xor_sync(0xffffffffu, npairs, o);
-    nfast += __shfl_xor_sync(0xffffffffu, nfast, o);
+    np += __shfl_xor_sync(0xffffffffu, np, o);
+    nf += __shfl_xor_sync(0xffffffffu, nf, o);
   }
-  if (lane == 0 && npairs) {
-    atomicAdd(&Q.counters[kPairs], npairs);
-    atomicAdd(&Q.counters[kPrunedFast], nfast);
+  if (lane == 0 && np) {
+    atomicAdd(&Q.counters[kPairs], np);
+    atomicAdd(&Q.counters[kPrunedFast], nf);
   }
 }
 
 }  // namespace
 
+size_t lb_smem_bytes() { return sizeof(LbShared); }
+
 void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
-               int tile_end, bool enumerate_all, cudaStream_t st) {
+               int tile_end, unsigned int* bits, bool enumerate_all, cudaStream_t st) {
   if (tile_end <= tile_begin) return;
-  k_lb<<<tile_end - tile_begin, kTileLags, 0, st>>>(S, Q, tiles + tile_begin, enumerate_all);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_lb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LbShared));
+    configured = true;
+  }
+  k_lb<<<tile_end - tile_begin, kLbThreads, sizeof(LbShared), st>>>(S, Q, tiles + tile_begin,
+                                                                     bits, enumerate_all);
 }
 
 }  // namespace dtwj

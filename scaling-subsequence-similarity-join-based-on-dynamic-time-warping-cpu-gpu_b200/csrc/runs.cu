@@ -7,7 +7,9 @@
 //   LB_Keogh        lb_keogh_stride_with_nomalise (raw-series envelope
 //                   normalised per window) GPU_version1/src/LB_keogh_warp.cu:74-96
 //
-// One warp owns one run (i0 + p, j0 + p), p < len.  Lane p of a batch of 32
+// Work items are (tile, lag) pairs of the diagonal sweep: a warp reads the
+// lag's survivor bits, cuts them into runs of consecutive rows (at most
+// kRunMax long) and owns each run (i0 + p, j0 + p), p < len.  Lane p of a batch of 32
 // holds pair p.  The masked bound needs six running sums along the diagonal;
 // their per-row increments are independent, so the warp computes all of a
 // batch's increments at once and turns them into the sums with one inclusive
@@ -85,26 +87,89 @@ __device__ __forceinline__ float keogh_term(float x, float U, float L) {
   return x > U ? du * du : (x < L ? dl * dl : 0.0f);
 }
 
-__global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch Q, bool masked,
+// Cuts the survivor bits of one lag into runs; returns how many runs were
+// written to `list` (at most `cap`) and advances *pos past them.
+__device__ int cut_runs(const unsigned int* w, int* pos, int2* list, int cap) {
+  int cnt = 0;
+  int p = *pos;
+  while (p < kLbRows && cnt < cap) {
+    const int wi = p >> 5, b = p & 31;
+    const unsigned int v = w[wi] >> b;
+    if (v == 0u) {
+      p = (wi + 1) << 5;
+      continue;
+    }
+    const int start = p + __ffs(v) - 1;
+    int e = start;
+    for (;;) {
+      const int wj = e >> 5, bj = e & 31;
+      const int ones = __ffs(~(w[wj] >> bj)) - 1;  // consecutive ones from bit bj
+      const int avail = 32 - bj;
+      if (ones < 0 || ones >= avail) {
+        e += avail;
+        if (e >= kLbRows) break;
+      } else {
+        e += ones;
+        break;
+      }
+    }
+    for (int r = start; r < e && cnt < cap; r += kRunMax) {
+      const int len = e - r < kRunMax ? e - r : kRunMax;
+      list[cnt++] = make_int2(r, len);
+      p = r + len;
+    }
+    if (p < e) break;  // list full in the middle of a run
+  }
+  *pos = p;
+  return cnt;
+}
+
+constexpr int kRunList = 32;
+
+__global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch Q,
+                                                         const Tile* tiles,
+                                                         const unsigned int* bits,
+                                                         unsigned int total_items, bool masked,
                                                          bool bounds) {
   __shared__ float offs[kRunWarps][2][kMaxWinBlocks];
+  __shared__ unsigned int wbits[kRunWarps][kLbWords];
+  __shared__ int2 rlist[kRunWarps][kRunList];
   __shared__ unsigned long long cnt[kNumCounters];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m = S.m, lo = kBias, hi = S.m - 1 - kBias;
   const int nblk = ((m - 1) >> kBlkShift) + 2;
   for (int x = threadIdx.x; x < kNumCounters; x += blockDim.x) cnt[x] = 0;
   __syncthreads();
-  const unsigned int total = *Q.run_count < Q.run_cap ? *Q.run_count : Q.run_cap;
   float* oi = offs[warp][0];
   float* oj = offs[warp][1];
+  unsigned int* wb = wbits[warp];
+  int2* rl = rlist[warp];
   for (;;) {
-    unsigned int idx = 0;
-    if (lane == 0) idx = atomicAdd(Q.run_next, 1u);
-    idx = __shfl_sync(0xffffffffu, idx, 0);
-    if (idx >= total) break;
-    const int4 R = Q.runs[idx];
-    const int64_t i0 = R.x, j0 = R.y;
-    const int len = R.z;
+    unsigned int item = 0;
+    if (lane == 0) item = atomicAdd(Q.run_next, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= total_items) break;
+    const unsigned int* src = bits + (size_t)item * kLbWords;
+    bool nz = false;
+    for (int x = lane; x < kLbWords; x += 32) {
+      const unsigned int v = src[x];
+      wb[x] = v;
+      nz |= v != 0u;
+    }
+    if (!__any_sync(0xffffffffu, nz)) continue;
+    __syncwarp();
+    const Tile T = tiles[item / kLbLags];
+    const int64_t L = (int64_t)T.L0 + (int64_t)(item % kLbLags);
+    int pos = 0;
+    for (;;) {
+      int nr = 0;
+      if (lane == 0) nr = cut_runs(wb, &pos, rl, kRunList);
+      nr = __shfl_sync(0xffffffffu, nr, 0);
+      __syncwarp();
+      if (nr == 0) break;
+      for (int ri = 0; ri < nr; ++ri) {
+    const int64_t i0 = (int64_t)T.i0 + rl[ri].x, j0 = i0 + L;
+    const int len = rl[ri].y;
     if (!bounds) {
       // no bounds: every pair of the run goes to the DTW stage
       for (int p = lane; p < len; p += 32) {
@@ -235,6 +300,9 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
       // a fresh best-so-far tightens the rest of the run
       thr = fminf(thr, prune_threshold_now(Q.bsf2, S.m));
     }
+      }
+      __syncwarp();
+    }
   }
   __syncthreads();
   for (int x = threadIdx.x; x < kNumCounters; x += blockDim.x)
@@ -281,12 +349,16 @@ void launch_center(const DevSeries& S, cudaStream_t st) {
   k_center<<<(unsigned)((S.n + 255) / 256), 256, 0, st>>>(S, nb);
 }
 
-void launch_runs(const DevSeries& S, const DevSearch& Q, bool masked, bool bounds, int num_sms,
+void launch_runs(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
+                 int tile_end, const unsigned int* bits, bool masked, bool bounds, int num_sms,
                  cudaStream_t st) {
+  if (tile_end <= tile_begin) return;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_runs, kRunWarps * 32, 0);
   if (per_sm < 1) per_sm = 1;
-  k_runs<<<num_sms * per_sm, kRunWarps * 32, 0, st>>>(S, Q, masked, bounds);
+  const unsigned int items = (unsigned int)(tile_end - tile_begin) * kLbLags;
+  k_runs<<<num_sms * per_sm, kRunWarps * 32, 0, st>>>(S, Q, tiles + tile_begin, bits, items,
+                                                       masked, bounds);
 }
 
 }  // namespace dtwj
