@@ -48,6 +48,7 @@ extern "C" {
 #define DTWJ_ERR_NODEVICE (-8)  /* no CUDA device                             */
 #define DTWJ_ERR_IO (-9)        /* file could not be read or written          */
 #define DTWJ_ERR_NOMODEL (-10)  /* learned ordering requested, no model loaded */
+#define DTWJ_ERR_SCRATCH (-11)  /* size exceeds the fixed scratch of dtwj_pair_dtw_noalloc */
 
 /* flags */
 #define DTWJ_F_NO_MASKED 0x1u   /* skip the masked diagonal bound             */
@@ -121,6 +122,26 @@ int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64
  * device (precise=0) or FP64 (precise=1).  dist[k] for (pi[k], pj[k]). */
 int dtwj_pair_dtw(const double* x, int64_t n, int32_t m, int32_t w, const int64_t* pi,
                   const int64_t* pj, int64_t count, int32_t precise, double* dist);
+
+/* Allocation-free variant of dtwj_pair_dtw for callers that must not allocate
+ * device memory (a host framework that reserves the device at start-up, a
+ * latency-bound loop that cannot take cudaMalloc's implicit synchronisation).
+ * No counterpart in the reference.  Everything is in device memory and owned
+ * by the caller: x_dev (n doubles), pi_dev / pj_dev (count int64 window
+ * indices), dist_dev (count doubles, the DTW distances; NaN for an index
+ * outside [0, s)).  Work is enqueued on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream) and not waited for.  The only scratch, the window
+ * statistics, is a fixed file-scope device array of 6.25 MiB holding at most
+ * DTWJ_NOALLOC_MAX_WINDOWS windows; larger series return DTWJ_ERR_SCRATCH.
+ * The array's device address is looked up on the first call on each device,
+ * with that device current, so make that first call before any stream
+ * capture.  Every call shares the array, so calls that overlap on the GPU
+ * (different streams, devices aside) race; it is rewritten by each call.
+ * Makes no cudaMalloc / cudaFree or other allocating call. */
+#define DTWJ_NOALLOC_MAX_WINDOWS 262144
+int dtwj_pair_dtw_noalloc(const double* x_dev, int64_t n, int32_t m, int32_t w,
+                          const int64_t* pi_dev, const int64_t* pj_dev, int64_t count,
+                          int32_t precise, double* dist_dev, void* stream);
 
 /* Band from a ratio: ceil(ratio*m) (rounding=0) or the reference's
  * max(round(ratio*m), 1) (rounding=1, GPU_version1/src/AAAA.cu:34). */

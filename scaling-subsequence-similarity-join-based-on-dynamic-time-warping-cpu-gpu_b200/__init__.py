@@ -33,6 +33,8 @@ ERR_TIMEOUT = -7
 ERR_NODEVICE = -8
 ERR_IO = -9
 ERR_NOMODEL = -10
+ERR_SCRATCH = -11
+NOALLOC_MAX_WINDOWS = 262144
 
 F_NO_MASKED = 0x1
 F_NO_SEED = 0x2
@@ -53,6 +55,7 @@ EXPORTS = (
     "dtwj_ctx_join_device",
     "dtwj_matrix_profile",
     "dtwj_pair_dtw",
+    "dtwj_pair_dtw_noalloc",
     "dtwj_band",
     "dtwj_strerror",
     "dtwj_device_count",
@@ -148,6 +151,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                                          P(_Result)]
     lib.dtwj_matrix_profile.argtypes = [P(d), i64, i32, P(d), P(i64)]
     lib.dtwj_pair_dtw.argtypes = [P(d), i64, i32, i32, P(i64), P(i64), i64, i32, P(d)]
+    vp = ctypes.c_void_p
+    lib.dtwj_pair_dtw_noalloc.argtypes = [vp, i64, i32, i32, vp, vp, i64, i32, vp, vp]
     lib.dtwj_band.argtypes = [i32, d, i32]
     lib.dtwj_band.restype = i32
     lib.dtwj_strerror.argtypes = [ctypes.c_int]

@@ -662,6 +662,7 @@ const char* dtwj_strerror(int code) {
     case DTWJ_ERR_NODEVICE: return "no CUDA device";
     case DTWJ_ERR_IO: return "file could not be read or written";
     case DTWJ_ERR_NOMODEL: return "learned ordering requested but no model is loaded";
+    case DTWJ_ERR_SCRATCH: return "series exceeds the fixed scratch of the allocation-free entry point";
     default: return "unknown error";
   }
 }

@@ -668,3 +668,96 @@ void launch_pair_dtw(const DevSeries& S, const int2* pairs, int count, bool prec
 }
 
 }  // namespace dtwj
+
+// ---- device-resident pair lists (allocation-free entry point) ----
+
+namespace dtwj {
+namespace {
+
+// Exact banded DTW distances (sqrt applied) of int64 pair lists that live in
+// device memory; a pair with an index outside [0, s) yields NaN.
+template <typename T, int C, int G>
+__global__ void __launch_bounds__(128) k_dtw_pairs64(DevSeries S, const int64_t* pi,
+                                                      const int64_t* pj, int64_t count,
+                                                      double* out, int group_elems) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
+  const int m = S.m, w = S.w;
+  const int gib = threadIdx.x / G, g = threadIdx.x % G;
+  const unsigned int gm = group_mask<G>();
+  const int groups = blockDim.x / G;
+  const int pq = G + 1, pt = G * C + G + 2;
+  T* q = sm + (size_t)gib * group_elems + pq;
+  T* t = q + m + pq + pt;
+  for (int x = g; x < pq; x += G) {
+    q[-1 - x] = Pad<T>::q();
+    q[m + x] = Pad<T>::q();
+  }
+  for (int x = g; x < pt; x += G) {
+    t[-1 - x] = Pad<T>::t();
+    t[m + x] = Pad<T>::t();
+  }
+  __syncwarp(gm);
+  for (int64_t k = (int64_t)blockIdx.x * groups + gib; k < count;
+       k += (int64_t)gridDim.x * groups) {
+    const int64_t i = pi[k], j = pj[k];
+    if (i < 0 || j < 0 || i >= S.s || j >= S.s) {
+      if (g == 0) out[k] = __longlong_as_double(0x7ff8000000000000LL);
+      continue;
+    }
+    const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
+    for (int x = g; x < m; x += G) {
+      q[x] = (T)((S.a[i + x] - mi) * si);
+      t[x] = (T)((S.a[j + x] - mj) * sj);
+    }
+    __syncwarp(gm);
+    unsigned long long cells;
+    bool ab;
+    const T d2 = dtw_band<T, C, G, false>(q, t, m, w, nullptr, 0, 0.0f, nullptr, gm, g, &cells,
+                                         &ab);
+    if (g == 0) out[k] = sqrt((double)d2);
+    __syncwarp(gm);
+  }
+}
+
+template <typename T, int C, int G>
+void run_pairs64(const DevSeries& S, const int64_t* pi, const int64_t* pj, int64_t count,
+                 double* out, cudaStream_t st) {
+  const int pq = G + 1, pt = G * C + G + 2;
+  const int elems = ((2 * pq + 2 * pt + 2 * S.m) + 3) & ~3;
+  int threads = 128;
+  size_t bytes = (size_t)(threads / G) * elems * sizeof(T);
+  while (bytes > 100 * 1024 && threads > G && threads > 32) {
+    threads /= 2;
+    bytes /= 2;
+  }
+  bytes = (size_t)(threads / G) * elems * sizeof(T);
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_dtw_pairs64<T, C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         200 * 1024);
+    configured = true;
+  }
+  const int groups = threads / G;
+  int64_t blocks = (count + groups - 1) / groups;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_dtw_pairs64<T, C, G><<<(unsigned)blocks, threads, bytes, st>>>(S, pi, pj, count, out, elems);
+}
+
+}  // namespace
+
+void launch_pair_dtw64(const DevSeries& S, const int64_t* pi, const int64_t* pj, int64_t count,
+                       bool precise, BandShape band, double* out, cudaStream_t st) {
+#define X(c, g)                                                 \
+  if (band.C == c && band.G == g) {                             \
+    if (precise)                                                \
+      run_pairs64<double, c, g>(S, pi, pj, count, out, st);     \
+    else                                                        \
+      run_pairs64<float, c, g>(S, pi, pj, count, out, st);      \
+  }
+  DTWJ_BAND_CASES(X)
+#undef X
+}
+
+}  // namespace dtwj

@@ -314,6 +314,10 @@ void launch_prep(const DevSeries& S, cudaStream_t st) {
   k_envelope<<<grid_for(S.n), kThreads, 0, st>>>(S);
 }
 
+void launch_stats(const DevSeries& S, cudaStream_t st) {
+  k_stats<<<grid_for(S.s), kThreads, 0, st>>>(S);
+}
+
 int mask_table_max(int m) {
   int z = (int)floor(sqrt((double)(m > 1 ? m - 1 : 1))) + 1;
   int lt = z * 200;
