@@ -175,11 +175,14 @@ void launch_rowterms(const DevSeries& S, bool masked, cudaStream_t st);
 int mask_table_max(int m);
 void launch_mask(const DevSeries& S, unsigned int* counts, int lt_max, double* diff,
                  double* mean_acc, float* zmax, cudaStream_t st);
+// Row minima over partners j >= i + m on LB tiles (lb.cu layout).
 void launch_mp(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long long* keys,
-               bool lower, cudaStream_t st);
+               cudaStream_t st);
+// Full profile: lo = row minima of the reversed series (nullptr: upper only).
 void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
                         const unsigned long long* lo, double* mp, int64_t* mpi,
                         cudaStream_t st);
+void launch_reverse(const double* a, int64_t n, double* out, cudaStream_t st);
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
                         unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st);
 // Fast diagonal bound over LB tiles [tile_begin, tile_end); survivors leave

@@ -54,8 +54,6 @@ struct dtwj_ctx {
   int num_sms = 0;
   std::vector<Buf> bufs;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  std::vector<Tile> tiles_host;      // 128-lag tiles of the ED profile
-  int64_t tiles_n = -1, tiles_m = -1;
   std::vector<Tile> lbtiles_host;    // kLbLags-lag tiles of the diagonal sweep
   int64_t lbtiles_n = -1, lbtiles_m = -1;
   std::vector<cudaEvent_t> pool;  // events for per-phase device times
@@ -66,7 +64,7 @@ namespace {
 enum BufId {
   B_A = 0, B_MU, B_SIG, B_ISG, B_FLAT, B_U, B_L, B_E, B_NU, B_DFA, B_DGA, B_DFE, B_DGE,
   B_AC, B_DUL, B_QSIG, B_MASK, B_MN, B_MDUL2, B_MDUL, B_SM, B_SME, B_STATUS,
-  B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_KEYS_LO, B_TILES, B_QUEUE, B_QCOUNT,
+  B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
   B_MP, B_MPI, B_CB, B_AF, B_UF, B_LF, B_BITS, B_LBTILES,
   B_COUNT_
@@ -155,26 +153,6 @@ int check_args(const void* x, int64_t n, int32_t m, int32_t w) {
   if (!x || m < 8 || w < 0) return DTWJ_ERR_ARG;
   if (n < 2 * (int64_t)m + 1 || n > (int64_t)INT32_MAX - 4) return DTWJ_ERR_ARG;
   return DTWJ_OK;
-}
-
-void build_tiles(dtwj_ctx* ctx, int64_t n, int m) {
-  if (ctx->tiles_n == n && ctx->tiles_m == m) return;
-  const int64_t s = n - m + 1;
-  ctx->tiles_host.clear();
-  int32_t order = 0;
-  for (int64_t L0 = m; L0 <= s - 1; L0 += kTileLags) {
-    const int64_t rows_total = s - L0;
-    for (int64_t i0 = 0; i0 < rows_total; i0 += kTileRows) {
-      Tile t;
-      t.L0 = (int32_t)L0;
-      t.i0 = (int32_t)i0;
-      t.rows = (int32_t)(rows_total - i0 < kTileRows ? rows_total - i0 : kTileRows);
-      t.order = order++;
-      ctx->tiles_host.push_back(t);
-    }
-  }
-  ctx->tiles_n = n;
-  ctx->tiles_m = m;
 }
 
 void build_lb_tiles(dtwj_ctx* ctx, int64_t n, int m) {
@@ -285,11 +263,12 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   if (rc) return rc;
   const int64_t s = S.s;
 
-  build_tiles(ctx, n, m);
-  const int ntiles = (int)ctx->tiles_host.size();
-  Tile* tiles;
-  ENSURE(B_TILES, (size_t)ntiles * sizeof(Tile), tiles);
-  CUDA_OK(cudaMemcpyAsync(tiles, ctx->tiles_host.data(), (size_t)ntiles * sizeof(Tile),
+  // tiles of the profile and the diagonal sweep (kLbLags lags x kLbRows rows)
+  build_lb_tiles(ctx, n, m);
+  const int nlb = (int)ctx->lbtiles_host.size();
+  Tile* lbtiles;
+  ENSURE(B_LBTILES, (size_t)nlb * sizeof(Tile), lbtiles);
+  CUDA_OK(cudaMemcpyAsync(lbtiles, ctx->lbtiles_host.data(), (size_t)nlb * sizeof(Tile),
                           cudaMemcpyHostToDevice, st));
 
   // search state
@@ -327,7 +306,7 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
     unsigned long long* keys;
     ENSURE(B_KEYS_UP, s * 8, keys);
     ph.begin();
-    launch_mp(S, tiles, ntiles, keys, false, st);
+    launch_mp(S, lbtiles, nlb, keys, st);
     ph.end(DTWJ_PHASE_PROFILE, 2);
     int2* seeds;
     unsigned int* nseeds;
@@ -347,12 +326,6 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   }
 
   // ---- diagonal sweep in chunks of LB tiles ----
-  build_lb_tiles(ctx, n, m);
-  const int nlb = (int)ctx->lbtiles_host.size();
-  Tile* lbtiles;
-  ENSURE(B_LBTILES, (size_t)nlb * sizeof(Tile), lbtiles);
-  CUDA_OK(cudaMemcpyAsync(lbtiles, ctx->lbtiles_host.data(), (size_t)nlb * sizeof(Tile),
-                          cudaMemcpyHostToDevice, st));
   const bool enumerate_all = flags & DTWJ_F_NO_DIAG;
   const double tile_pairs = (double)kLbLags * kLbRows;
   int chunk = kLbChunkTiles;
@@ -559,29 +532,48 @@ int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64
   if (!mp || !mpi) return DTWJ_ERR_ARG;
   int rc = check_args(x, n, m, 0);
   if (rc) return rc;
+  // Row minima over partners j >= i + m come from the series, those over
+  // j <= i - m from the reversed series: reversing both windows keeps their
+  // z-normalised distance, and window i becomes window s-1-i.
   dtwj_ctx* ctx = nullptr;
+  dtwj_ctx* rev = nullptr;
   rc = dtwj_ctx_create(0, &ctx);
   if (rc) return rc;
+  rc = dtwj_ctx_create(0, &rev);
+  if (rc) {
+    dtwj_ctx_destroy(ctx);
+    return rc;
+  }
   do {
     double* dev = nullptr;
     if ((rc = upload(ctx, x, n, &dev))) break;
-    DevSeries S;
-    if ((rc = prepare(ctx, dev, n, m, 0, false, &S))) break;
-    build_tiles(ctx, n, m);
-    const int ntiles = (int)ctx->tiles_host.size();
-    Tile* tiles;
     void* p;
-    if ((rc = ensure(ctx, B_TILES, (size_t)ntiles * sizeof(Tile), &p))) break;
-    tiles = (Tile*)p;
-    cudaMemcpyAsync(tiles, ctx->tiles_host.data(), (size_t)ntiles * sizeof(Tile),
-                    cudaMemcpyHostToDevice, ctx->stream);
+    if ((rc = ensure(rev, B_A, n * 8, &p))) break;
+    double* rdev = (double*)p;
+    launch_reverse(dev, n, rdev, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      rc = DTWJ_ERR_CUDA;
+      break;
+    }
+    DevSeries S, R;
+    if ((rc = prepare(ctx, dev, n, m, 0, false, &S))) break;
+    if ((rc = prepare(rev, rdev, n, m, 0, false, &R))) break;
+    build_lb_tiles(ctx, n, m);
+    const int nlb = (int)ctx->lbtiles_host.size();
+    if ((rc = ensure(ctx, B_LBTILES, (size_t)nlb * sizeof(Tile), &p))) break;
+    Tile* tiles = (Tile*)p;
+    cudaMemcpy(tiles, ctx->lbtiles_host.data(), (size_t)nlb * sizeof(Tile), cudaMemcpyHostToDevice);
     const int64_t s = n - m + 1;
     if ((rc = ensure(ctx, B_KEYS_UP, s * 8, &p))) break;
     unsigned long long* up = (unsigned long long*)p;
-    if ((rc = ensure(ctx, B_KEYS_LO, s * 8, &p))) break;
+    if ((rc = ensure(rev, B_KEYS_UP, s * 8, &p))) break;
     unsigned long long* lo = (unsigned long long*)p;
-    launch_mp(S, tiles, ntiles, up, false, ctx->stream);
-    launch_mp(S, tiles, ntiles, lo, true, ctx->stream);
+    launch_mp(S, tiles, nlb, up, ctx->stream);
+    launch_mp(R, tiles, nlb, lo, rev->stream);
+    if (cudaStreamSynchronize(rev->stream) != cudaSuccess) {
+      rc = DTWJ_ERR_CUDA;
+      break;
+    }
     if ((rc = ensure(ctx, B_MP, s * 8, &p))) break;
     double* dmp = (double*)p;
     if ((rc = ensure(ctx, B_MPI, s * 8, &p))) break;
@@ -594,6 +586,7 @@ int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64
       break;
     }
   } while (0);
+  dtwj_ctx_destroy(rev);
   dtwj_ctx_destroy(ctx);
   return rc;
 }

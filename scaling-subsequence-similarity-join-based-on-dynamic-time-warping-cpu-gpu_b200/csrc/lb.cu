@@ -110,33 +110,23 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_lb(DevSeries S, DevSearch Q,
     __syncthreads();
     for (int x = t; x < kCols; x += kLbThreads) {
       const int64_t j = c0 + x;
-      if (j >= 1 && j < s) {
-        sh.p1[x] = S.dfa[j - 1];
-        sh.p2[x] = S.dga[j - 1];
-        sh.p3[x] = S.dfE[j - 1];
-        sh.p4[x] = S.dgE[j - 1];
-        sh.sg[x] = S.sig[j];
-        sh.g[x] = g_of(S, j, twoB);
-      } else {
-        sh.p1[x] = sh.p2[x] = sh.p3[x] = sh.p4[x] = 0.0;
-        sh.sg[x] = 1.0;
-        sh.g[x] = 1e300;
-      }
+      const bool in = j >= 0 && j < s, up = j >= 1 && j < s;  // update terms exist for j >= 1
+      sh.p1[x] = up ? S.dfa[j - 1] : 0.0;
+      sh.p2[x] = up ? S.dga[j - 1] : 0.0;
+      sh.p3[x] = up ? S.dfE[j - 1] : 0.0;
+      sh.p4[x] = up ? S.dgE[j - 1] : 0.0;
+      sh.sg[x] = in ? S.sig[j] : 1.0;
+      sh.g[x] = in ? g_of(S, j, twoB) : 1e300;
     }
     for (int x = t; x < kStage; x += kLbThreads) {
       const int64_t i = r0 + x;
-      if (i >= 1 && i < s) {
-        sh.r1[x] = S.dfa[i - 1];
-        sh.r2[x] = S.dga[i - 1];
-        sh.r3[x] = S.dfE[i - 1];
-        sh.r4[x] = S.dgE[i - 1];
-        sh.rs[x] = S.sig[i];
-        sh.rg[x] = g_of(S, i, twoB);
-      } else {
-        sh.r1[x] = sh.r2[x] = sh.r3[x] = sh.r4[x] = 0.0;
-        sh.rs[x] = 1.0;
-        sh.rg[x] = 1e300;
-      }
+      const bool in = i >= 0 && i < s, up = i >= 1 && i < s;
+      sh.r1[x] = up ? S.dfa[i - 1] : 0.0;
+      sh.r2[x] = up ? S.dga[i - 1] : 0.0;
+      sh.r3[x] = up ? S.dfE[i - 1] : 0.0;
+      sh.r4[x] = up ? S.dgE[i - 1] : 0.0;
+      sh.rs[x] = in ? S.sig[i] : 1.0;
+      sh.rg[x] = in ? g_of(S, i, twoB) : 1e300;
     }
     __syncthreads();
     // windows: column of lag l at stage row 0 is stage column t*K + l

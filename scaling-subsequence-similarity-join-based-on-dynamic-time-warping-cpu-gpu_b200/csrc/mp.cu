@@ -26,71 +26,132 @@ namespace {
 
 constexpr int kMpRowsMax = 4096;
 
-// LOWER = false: pairs (r, r + L), reduction to row r  (j > i neighbours)
-// LOWER = true:  pairs (r, r - L), reduction to row r  (j < i neighbours)
-template <bool LOWER>
-__global__ void __launch_bounds__(kTileLags) k_mp(DevSeries S, const Tile* tiles,
-                                                  unsigned long long* keys) {
-  __shared__ unsigned long long rowbest[kMpRowsMax];
+// Row minima of ED^2 over the upper triangle (partners j >= i + m).  Tile and
+// staging as in the diagonal sweep (lb.cu): 128 threads x kLbPerThread lags
+// x kLbRows rows, column operands (df[j-1], dg[j-1], 1/sig_j and the flat
+// guard 2m | 1e300) staged per kStage rows in shared memory and slid through
+// registers.  Per row a thread keeps its best of kLbPerThread lags, the warp
+// reduces the high words with one REDUX, and the winner lane folds its key
+// into the tile's row minima with a shared 64-bit atomicMin.
+constexpr int kStage = kLbPerThread * 32;
+constexpr int kCols = kLbLags + kStage;
+
+struct MpShared {
+  double p1[kCols], p2[kCols], is[kCols], c2[kCols];
+  double r1[kStage], r2[kStage], ci[kStage];
+  unsigned long long rowbest[kLbRows];
+};
+
+__global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* tiles,
+                                                      unsigned long long* keys) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  MpShared& sh = *reinterpret_cast<MpShared*>(smraw);
   const Tile T = tiles[blockIdx.x];
-  const int64_t L = (int64_t)T.L0 + threadIdx.x;
   const int64_t s = S.s;
   const int m = S.m;
-  // rows of this tile (upper: i; lower: r = i + L0)
-  const int64_t rbase = LOWER ? (int64_t)T.L0 + T.i0 : (int64_t)T.i0;
-  const int rows = T.rows;
-  for (int x = threadIdx.x; x < rows; x += blockDim.x) rowbest[x] = ULLONG_MAX;
-  __syncthreads();
+  const int t = threadIdx.x, lane = t & 31;
+  const int64_t L0 = T.L0, i0 = T.i0;
+  const int64_t Lt = L0 + (int64_t)t * kLbPerThread;
+  for (int x = t; x < T.rows; x += kLbThreads) sh.rowbest[x] = ULLONG_MAX;
 
-  int64_t r_start, r_end;  // this thread's rows [r_start, r_end)
-  if (LOWER) {
-    r_start = rbase > L ? rbase : L;
-    r_end = rbase + rows < s ? rbase + rows : s;
-  } else {
-    r_start = rbase;
-    r_end = rbase + rows < s - L ? rbase + rows : s - L;
-  }
-  const bool any = L < s && r_start < r_end;
-
-  double C = 0.0;
-  if (any) {
-    const int64_t c0 = LOWER ? r_start - L : r_start + L;
-    const double mr = S.mu[r_start], mc = S.mu[c0];
-    for (int k = 0; k < m; ++k) C = fma(S.a[r_start + k] - mr, S.a[c0 + k] - mc, C);
-  }
-  const int lane = threadIdx.x & 31;
-  for (int x = 0; x < rows; ++x) {
-    const int64_t r = rbase + x;
-    unsigned int hi = UINT_MAX;
-    int64_t c = 0;
-    if (any && r >= r_start && r < r_end) {
-      c = LOWER ? r - L : r + L;
-      if (r > r_start) {
-        C = fma(S.dfa[r - 1], S.dga[c - 1], C);
-        C = fma(S.dfa[c - 1], S.dga[r - 1], C);
-      }
-      if (!S.flat[r] && !S.flat[c]) {
-        double e2 = fma(-2.0 * C * S.isg[r], S.isg[c], 2.0 * m);
-        e2 = fmax(e2, 0.0);
-        hi = (unsigned int)__double2hiint(e2);
-      }
+  // exact anchors C(i0, i0 + L) for the thread's lags
+  double C[kLbPerThread];
+  {
+    double mj[kLbPerThread], wa[kLbPerThread];
+    const int64_t jb = i0 + Lt;
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) {
+      C[l] = 0.0;
+      mj[l] = S.mu[jb + l < s ? jb + l : s - 1];
+      wa[l] = S.a[jb + l < S.n ? jb + l : S.n - 1];
     }
-    const unsigned int best = __reduce_min_sync(0xffffffffu, hi);
-    if (best != UINT_MAX) {
-      const unsigned int ballot = __ballot_sync(0xffffffffu, hi == best);
-      // lowest partner index: lowest lane (upper) or highest lane (lower)
-      const int win = LOWER ? 31 - __clz(ballot) : __ffs(ballot) - 1;
-      if (lane == win) {
-        const unsigned long long key =
-            ((unsigned long long)best << 32) | (unsigned long long)(unsigned int)c;
-        atomicMin(&rowbest[x], key);
-      }
+    const double mi = S.mu[i0];
+    for (int k = 0; k < m; ++k) {
+      const double ai = S.a[i0 + k] - mi;
+#pragma unroll
+      for (int l = 0; l < kLbPerThread; ++l) C[l] = fma(ai, wa[l] - mj[l], C[l]);
+#pragma unroll
+      for (int l = 0; l < kLbPerThread - 1; ++l) wa[l] = wa[l + 1];
+      const int64_t x = jb + kLbPerThread + k < S.n ? jb + kLbPerThread + k : S.n - 1;
+      wa[kLbPerThread - 1] = S.a[x];
     }
   }
+  double w1[kLbPerThread], w2[kLbPerThread], wi[kLbPerThread], wc[kLbPerThread];
+  const double two_m = 2.0 * m;
+  for (int st = 0; st < T.rows; st += kStage) {
+    const int64_t r0 = i0 + st, c0 = r0 + L0;
+    __syncthreads();
+    for (int x = t; x < kCols; x += kLbThreads) {
+      const int64_t j = c0 + x;
+      const bool in = j >= 0 && j < s, up = j >= 1 && j < s;  // update terms exist for j >= 1
+      sh.p1[x] = up ? S.dfa[j - 1] : 0.0;
+      sh.p2[x] = up ? S.dga[j - 1] : 0.0;
+      sh.is[x] = in ? S.isg[j] : 0.0;
+      sh.c2[x] = (in && !S.flat[j]) ? two_m : 1e300;
+    }
+    for (int x = t; x < kStage; x += kLbThreads) {
+      const int64_t i = r0 + x;
+      const bool in = i >= 0 && i < s, up = i >= 1 && i < s;
+      sh.r1[x] = up ? S.dfa[i - 1] : 0.0;
+      sh.r2[x] = up ? S.dga[i - 1] : 0.0;
+      sh.ci[x] = (in && !S.flat[i]) ? -2.0 * S.isg[i] : 0.0;
+    }
+    __syncthreads();
+    const int cb = t * kLbPerThread;
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) {
+      w1[l] = sh.p1[cb + l];
+      w2[l] = sh.p2[cb + l];
+      wi[l] = sh.is[cb + l];
+      wc[l] = sh.c2[cb + l];
+    }
+    for (int qq = 0; qq < kStage / kLbPerThread; ++qq) {
+#pragma unroll
+      for (int u = 0; u < kLbPerThread; ++u) {
+        const int r = qq * kLbPerThread + u;
+        const int64_t i = r0 + r;
+        const bool first = (st == 0 && r == 0);
+        const double q1 = sh.r1[r], q2 = sh.r2[r], qc = sh.ci[r];
+        unsigned int best = UINT_MAX;
+        int bl = 0;
+#pragma unroll
+        for (int l = 0; l < kLbPerThread; ++l) {
+          const int sl = (u + l) % kLbPerThread;
+          if (!first) {
+            C[l] = fma(q1, w2[sl], C[l]);
+            C[l] = fma(w1[sl], q2, C[l]);
+          }
+          const double e2 = fmax(fma(C[l] * qc, wi[sl], wc[sl]), 0.0);
+          const unsigned int hi = (unsigned int)__double2hiint(e2);
+          const bool ok = (st + r < T.rows) && (i + Lt + l < s);
+          if (ok && hi < best) {
+            best = hi;
+            bl = l;
+          }
+        }
+        const int nx = cb + r + kLbPerThread;
+        w1[u] = sh.p1[nx];
+        w2[u] = sh.p2[nx];
+        wi[u] = sh.is[nx];
+        wc[u] = sh.c2[nx];
+        if (qc != 0.0) {  // flat rows have no neighbour
+          const unsigned int wbest = __reduce_min_sync(0xffffffffu, best);
+          if (wbest != UINT_MAX) {
+            const unsigned int ballot = __ballot_sync(0xffffffffu, best == wbest);
+            if (lane == __ffs(ballot) - 1) {
+              const unsigned long long key =
+                  ((unsigned long long)wbest << 32) | (unsigned long long)(unsigned int)(i + Lt + bl);
+              atomicMin(&sh.rowbest[st + r], key);
+            }
+          }
+        }
+      }
+    }
+  }
   __syncthreads();
-  for (int x = threadIdx.x; x < rows; x += blockDim.x) {
-    const unsigned long long v = rowbest[x];
-    if (v != ULLONG_MAX) atomicMin(&keys[rbase + x], v);
+  for (int x = t; x < T.rows; x += kLbThreads) {
+    const unsigned long long v = sh.rowbest[x];
+    if (v != ULLONG_MAX) atomicMin(&keys[i0 + x], v);
   }
 }
 
@@ -107,7 +168,11 @@ __global__ void k_mp_finalize(DevSeries S, const unsigned long long* up,
   if (i >= S.s) return;
   unsigned long long k = up[i];
   if (lo) {
-    const unsigned long long k2 = lo[i];
+    // lo holds the row minima of the reversed series: row s-1-i, partner s-1-j
+    unsigned long long k2 = lo[S.s - 1 - i];
+    if (k2 != ULLONG_MAX)
+      k2 = (k2 & 0xffffffff00000000ull) |
+           (unsigned long long)(unsigned int)(S.s - 1 - (int64_t)(k2 & 0xffffffffu));
     // tie on the distance key: lowest partner index
     if ((k2 >> 32) < (k >> 32) || ((k2 >> 32) == (k >> 32) && (k2 & 0xffffffffu) < (k & 0xffffffffu)))
       k = k2;
@@ -215,20 +280,31 @@ __global__ void __launch_bounds__(kSelThreads) k_seed_select(DevSeries S,
   if (threadIdx.x == 0) *nseeds = count;
 }
 
+__global__ void k_reverse(const double* a, int64_t n, double* out) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x)
+    out[p] = a[n - 1 - p];
+}
+
 }  // namespace
 
+void launch_reverse(const double* a, int64_t n, double* out, cudaStream_t st) {
+  k_reverse<<<1024, 256, 0, st>>>(a, n, out);
+}
+
 void launch_mp(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long long* keys,
-               bool lower, cudaStream_t st) {
+               cudaStream_t st) {
   k_fill_u64<<<1024, 256, 0, st>>>(keys, S.s, ULLONG_MAX);
   if (ntiles <= 0) return;
-  // grid limit is 2^31-1 blocks; tiles are launched in slabs to stay far below
+  static bool configured = false;
+  if (!configured) {
+    cudaFuncSetAttribute(k_mp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MpShared));
+    configured = true;
+  }
   const int slab = 1 << 20;
   for (int b = 0; b < ntiles; b += slab) {
     const int cnt = ntiles - b < slab ? ntiles - b : slab;
-    if (lower)
-      k_mp<true><<<cnt, kTileLags, 0, st>>>(S, tiles + b, keys);
-    else
-      k_mp<false><<<cnt, kTileLags, 0, st>>>(S, tiles + b, keys);
+    k_mp<<<cnt, kLbThreads, sizeof(MpShared), st>>>(S, tiles + b, keys);
   }
 }
 

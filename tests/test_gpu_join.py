@@ -13,11 +13,12 @@ from conftest import PKG_DIR
 pytestmark = pytest.mark.gpu
 
 REL = 1e-5
+ABS_ZERO = 1e-9  # distances of exact copies are rounding noise around 0
 
 
 def _check(r, i, j, dist, what=""):
     assert (r.i, r.j) == (i, j), what
-    assert abs(r.dist - dist) <= REL * max(dist, 1e-12), (what, r.dist, dist)
+    assert abs(r.dist - dist) <= max(REL * dist, ABS_ZERO), (what, r.dist, dist)
 
 
 def test_golden_reference_joins(gpu_dtwj, golden):
@@ -133,3 +134,22 @@ def test_cli_drop_in(tmp_path, golden):
     assert "final distance :%f" % c["dist"] in out
     lines = tf.read_text().splitlines()
     assert len(lines) == 2 and lines[0] == "1.5" and float(lines[1]) > 0
+
+
+@pytest.mark.parametrize("where", ["first", "last"])
+def test_best_pair_at_the_series_ends(gpu_dtwj, oracle, synth, where):
+    # the first window (row 0 of every diagonal) and the last window (last
+    # column) must be reachable by the sweep
+    x = synth.random_walk(4000, 12)
+    m, w = 96, 5
+    s = x.size - m + 1
+    if where == "first":
+        x[2100:2100 + m] = x[0:m] * 1.5 + 7.0   # z-normalised copy of window 0
+        expect = (0, 2100)
+    else:
+        x[s - 1:s - 1 + m] = x[1300:1300 + m] - 2.0  # copy of window 1300 at the end
+        expect = (1300, s - 1)
+    ref = oracle.join(x, m, w)
+    r = gpu_dtwj.join(x, m, w)
+    assert (ref.i, ref.j) == expect
+    _check(r, ref.i, ref.j, ref.dist)
