@@ -187,6 +187,11 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_lb(DevSeries S, DevSearch Q,
       }
     }
   }
+  // words past the tile's last stage (short tiles) are zero, never stale
+  for (int wi = ((T.rows + kStage - 1) / kStage) * (kStage / 32); wi < kLbWords; ++wi) {
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) out[(size_t)(t * kLbPerThread + l) * kLbWords + wi] = 0u;
+  }
   unsigned long long np = npairs, nf = nfast;
   for (int o = 16; o > 0; o >>= 1) {
     np += __shfl_xor_sync(0xffffffffu, np, o);

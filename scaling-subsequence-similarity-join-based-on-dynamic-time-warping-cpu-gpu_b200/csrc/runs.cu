@@ -150,16 +150,22 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= total_items) break;
     const unsigned int* src = bits + (size_t)item * kLbWords;
+    const Tile T = tiles[item / kLbLags];
+    const int64_t L = (int64_t)T.L0 + (int64_t)(item % kLbLags);
+    // rows this lag really has in the tile: r < rows and i0 + r + L < s
+    int64_t nrow = S.s - L - T.i0;
+    if (nrow > T.rows) nrow = T.rows;
     bool nz = false;
     for (int x = lane; x < kLbWords; x += 32) {
-      const unsigned int v = src[x];
+      unsigned int v = src[x];
+      const int64_t lo_row = (int64_t)x * 32;
+      if (lo_row >= nrow) v = 0u;
+      else if (lo_row + 32 > nrow) v &= (1u << (nrow - lo_row)) - 1u;
       wb[x] = v;
       nz |= v != 0u;
     }
     if (!__any_sync(0xffffffffu, nz)) continue;
     __syncwarp();
-    const Tile T = tiles[item / kLbLags];
-    const int64_t L = (int64_t)T.L0 + (int64_t)(item % kLbLags);
     int pos = 0;
     for (;;) {
       int nr = 0;

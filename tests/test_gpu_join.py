@@ -153,3 +153,20 @@ def test_best_pair_at_the_series_ends(gpu_dtwj, oracle, synth, where):
     r = gpu_dtwj.join(x, m, w)
     assert (ref.i, ref.j) == expect
     _check(r, ref.i, ref.j, ref.dist)
+
+
+def test_context_reuse_leaves_no_stale_state(gpu_dtwj, oracle, synth):
+    # a larger, survivor-rich join first, then smaller ones on the same
+    # context: every result must equal a fresh join and the stage counts must
+    # stay consistent (no pair is examined that the diagonal bound dropped)
+    big = synth.ecg_like(12000, 5)
+    xs = [(synth.random_walk(7000, 21), 128, 7), (synth.random_walk(4500, 22), 64, 3)]
+    with gpu_dtwj.Context() as ctx:
+        ctx.join(big, 128, 7)
+        for x, m, w in xs:
+            r = ctx.join(x, m, w)
+            ref = oracle.join(x, m, w)
+            _check(r, ref.i, ref.j, ref.dist)
+            later = r.pruned_masked + r.pruned_kim + r.pruned_keogh + r.dtw_calls
+            assert later <= r.pairs - r.pruned_fast + 2 * 100, (later, r.pairs - r.pruned_fast)
+            assert 0 <= r.i < r.j < x.size - m + 1
