@@ -246,7 +246,10 @@ def run_ours(args):
     else:
         raise SystemExit("bench.py needs torch with CUDA for device buffers")
     ctx = dtwj.Context(local)
-    flags = 0
+    # F_PROFILE records CUDA events around every launch group on the join's
+    # stream (no synchronisation), so the timed joins also give the per-phase
+    # device times the roofline uses.
+    flags = dtwj.F_PROFILE
     for _ in range(args.warmup):
         ctx.join_device(dptr, n, m, w, flags)
     _barrier(dist)
@@ -263,10 +266,11 @@ def run_ours(args):
     r0 = results[-1]
     value = world * pairs_total * args.steps / dev_seconds
 
-    # profiled pass: per-phase device time for the roofline (same workload)
-    prof = ctx.join_device(dptr, n, m, w, flags | dtwj.F_PROFILE)
-    phases = dict(zip(dtwj.PHASES, prof.phase_seconds[:len(dtwj.PHASES)]))
-    launches = dict(zip(dtwj.PHASES, prof.phase_launches[:len(dtwj.PHASES)]))
+    # per-phase device time and launches, averaged over the timed joins
+    phases = {p: sum(r.phase_seconds[k] for r in results) / args.steps
+              for k, p in enumerate(dtwj.PHASES)}
+    launches = {p: sum(r.phase_launches[k] for r in results) / args.steps
+                for k, p in enumerate(dtwj.PHASES)}
     dominant = max(phases, key=phases.get)
 
     # e2e through the host-pointer API (pinned host buffer)
@@ -320,7 +324,7 @@ def run_ours(args):
                 cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
                        "sample": "first %d samples, oracle C restatement, %.1f s"
                                  % (args.cpu_sample, cw)}
-    gpu_launches = int(sum(prof.phase_launches[:len(dtwj.PHASES)])) * args.steps
+    gpu_launches = int(sum(launches.values()) * args.steps)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * dev_seconds / args.steps,
