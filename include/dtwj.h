@@ -50,6 +50,10 @@ extern "C" {
 #define DTWJ_ERR_NOMODEL (-10)  /* learned ordering requested, no model loaded */
 #define DTWJ_ERR_SCRATCH (-11)  /* size exceeds the fixed scratch of dtwj_pair_dtw_noalloc */
 
+/* longest subsequence the joins accept (62 blocks of 1024 samples); longer m
+ * returns DTWJ_ERR_ARG */
+#define DTWJ_MAX_M 63488
+
 /* flags */
 #define DTWJ_F_NO_MASKED 0x1u   /* skip the masked diagonal bound             */
 #define DTWJ_F_NO_SEED 0x2u     /* no ED-profile seeding of the best-so-far   */
@@ -65,8 +69,9 @@ extern "C" {
 #define DTWJ_PHASE_DIAG 3       /* diagonal bound sweep                       */
 #define DTWJ_PHASE_PAIRS 4      /* LB_Keogh with cumulative bound + DTW       */
 #define DTWJ_PHASE_VERIFY 5     /* FP64 re-verification                       */
-#define DTWJ_PHASE_RUNS 6       /* masked / endpoint / LB_Keogh on runs       */
-#define DTWJ_NUM_PHASES 7
+#define DTWJ_PHASE_RUNS 6       /* masked / endpoint bounds on runs           */
+#define DTWJ_PHASE_KEOGH 7      /* LB_Keogh on the run filter's survivors     */
+#define DTWJ_NUM_PHASES 8
 
 typedef struct {
   int64_t i, j;            /* top-1 pair, 0-based, j - i >= m                */

@@ -43,7 +43,7 @@ F_LEARNED = 0x8
 F_VERBOSE = 0x10
 F_PROFILE = 0x20
 
-PHASES = ("prep", "profile", "seeds", "diag", "pairs", "verify", "runs")
+PHASES = ("prep", "profile", "seeds", "diag", "pairs", "verify", "runs", "keogh")
 
 # Every symbol include/dtwj.h declares.
 EXPORTS = (

@@ -109,8 +109,7 @@ struct DevSeries {
   double* SME;      // s, sum_T M E
   double* cb;       // (n >> kBlkShift) + 2, block centers
   float* af;        // n, a - cb[block]
-  float* Uf;        // n, U - cb[block]
-  float* Lf;        // n, L - cb[block]
+  float2* crf;      // n, ((U + L) / 2 - cb[block], (U - L) / 2): envelope center, radius
   int* status;      // device status word (0 ok, else error bits)
 };
 
@@ -129,6 +128,10 @@ struct DevSearch {
   unsigned int* queue_count;
   unsigned int* queue_next;
   unsigned int queue_cap;
+  int4* kq;                     // LB_Keogh candidates: (i, j, endpoint bound bits, 0)
+  unsigned int* kq_count;
+  unsigned int* kq_next;
+  unsigned int kq_cap;
 };
 
 // Endpoint bound: minimum cost of any warping path's cells in the first and
@@ -197,6 +200,9 @@ void launch_runs(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int 
                  int tile_end, const unsigned int* bits, bool masked, bool bounds, int num_sms,
                  cudaStream_t st);
 void launch_center(const DevSeries& S, cudaStream_t st);
+// LB_Keogh over the candidates the run filter queued in Q.kq; survivors go to
+// Q.queue.
+void launch_keogh(const DevSeries& S, const DevSearch& Q, int num_sms, cudaStream_t st);
 // bounds = false: DTW only (the seeds); true: endpoint bound + LB_Keogh first
 void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
                   const unsigned int* npairs, bool bounds, BandShape band, int num_sms,

@@ -66,7 +66,7 @@ enum BufId {
   B_AC, B_DUL, B_QSIG, B_MASK, B_MN, B_MDUL2, B_MDUL, B_SM, B_SME, B_STATUS,
   B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
-  B_MP, B_MPI, B_CB, B_AF, B_UF, B_LF, B_BITS, B_LBTILES,
+  B_MP, B_MPI, B_CB, B_AF, B_CRF, B_BITS, B_LBTILES, B_KQ,
   B_COUNT_
 };
 
@@ -150,7 +150,7 @@ struct Phases {
 };
 
 int check_args(const void* x, int64_t n, int32_t m, int32_t w) {
-  if (!x || m < 8 || w < 0) return DTWJ_ERR_ARG;
+  if (!x || m < 8 || m > DTWJ_MAX_M || w < 0) return DTWJ_ERR_ARG;
   if (n < 2 * (int64_t)m + 1 || n > (int64_t)INT32_MAX - 4) return DTWJ_ERR_ARG;
   return DTWJ_OK;
 }
@@ -209,8 +209,7 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   ENSURE(B_SME, s * 8, S.SME);
   ENSURE(B_CB, ((n >> kBlkShift) + 4) * 8, S.cb);
   ENSURE(B_AF, n * 4, S.af);
-  ENSURE(B_UF, n * 4, S.Uf);
-  ENSURE(B_LF, n * 4, S.Lf);
+  ENSURE(B_CRF, n * 8, S.crf);
   ENSURE(B_STATUS, 4, S.status);
   cudaStream_t st = ctx->stream;
   CUDA_OK(cudaMemsetAsync(S.status, 0, 4, st));
@@ -280,13 +279,18 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
     if (v >= 1024 && v < (long)kQueueCapMax) qcap = (unsigned int)v;
   }
   ENSURE(B_QUEUE, (size_t)qcap * sizeof(int2), Q.queue);
+  // LB_Keogh candidates of one chunk: twice the DTW queue (most are pruned)
+  ENSURE(B_KQ, (size_t)qcap * 2 * sizeof(int4), Q.kq);
   unsigned int* qc;
-  ENSURE(B_QCOUNT, 16, qc);
+  ENSURE(B_QCOUNT, 32, qc);
   Q.queue_count = qc;
   Q.queue_next = qc + 1;
   Q.run_count = qc + 2;
   Q.run_next = qc + 3;
+  Q.kq_count = qc + 4;
+  Q.kq_next = qc + 5;
   Q.queue_cap = qcap;
+  Q.kq_cap = qcap * 2;
   Q.runs = nullptr;
   Q.run_cap = 0;
   ENSURE(B_BSF2, 4, Q.bsf2);
@@ -335,13 +339,18 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   for (int attempt = 0;; ++attempt) {
     for (int t0 = 0; t0 < nlb; t0 += chunk) {
       const int t1 = t0 + chunk < nlb ? t0 + chunk : nlb;
-      CUDA_OK(cudaMemsetAsync(qc, 0, 16, st));
+      CUDA_OK(cudaMemsetAsync(qc, 0, 32, st));
       ph.begin();
       launch_lb(S, Q, lbtiles, t0, t1, bits, enumerate_all, st);
       ph.end(DTWJ_PHASE_DIAG, 1);
       ph.begin();
       launch_runs(S, Q, lbtiles, t0, t1, bits, masked, !enumerate_all, ctx->num_sms, st);
       ph.end(DTWJ_PHASE_RUNS, 1);
+      if (!enumerate_all) {
+        ph.begin();
+        launch_keogh(S, Q, ctx->num_sms, st);
+        ph.end(DTWJ_PHASE_KEOGH, 1);
+      }
       ph.begin();
       launch_pairs(S, Q, Q.queue, Q.queue_count, true, band, ctx->num_sms, st);
       ph.end(DTWJ_PHASE_PAIRS, 1);

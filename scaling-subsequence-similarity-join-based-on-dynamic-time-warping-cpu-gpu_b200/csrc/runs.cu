@@ -16,18 +16,23 @@
 // scan, anchored by an exact O(m) evaluation at the run's first pair (FP64
 // throughout, as in the reference's recurrence).  The endpoint bound is one
 // lane's work per pair.  LB_Keogh then runs pair by pair with the lanes
-// spread over positions, in rounds of 256 positions that stop as soon as
-// either direction exceeds the best-so-far; the run's windows overlap, so
+// spread over positions, one direction at a time (the second only when the
+// first stays within the best-so-far), checking the warp's running sum every
+// kKeoghCheck samples; most pairs that reach it are pruned within the first
+// few hundred samples of the first direction.  The run's windows overlap, so
 // consecutive pairs re-read the same lines from L1.  It reads FP32 copies of
-// the series and envelope centered per 1024-sample block, normalised per
-// window.  Survivors go to the DTW queue.
+// the series and of the envelope as (center, radius), centered per
+// 1024-sample block and normalised per window.  Survivors go to the DTW queue.
+#include "../../include/dtwj.h"
 #include "dtwj_dev.cuh"
 
 namespace dtwj {
 namespace {
 
 constexpr int kRunWarps = 4;
-constexpr int kMaxWinBlocks = 64;  // windows up to 62 * 1024 samples
+constexpr int kKeoghCheck = 128;  // samples between two best-so-far checks of LB_Keogh
+constexpr int kKeoghWarps = 8;    // warps per block of the LB_Keogh kernel
+constexpr int kKeoghBatch = 8;    // consecutive queue entries a warp takes at once
 
 // Masked bound for env = r, query = c from the raw FP64 sums
 // F1 = sum_T M_r a_c, F2 = sum_T M_r a_c^2, F3 = sum_T M_r E_r a_c.
@@ -82,9 +87,88 @@ __device__ __forceinline__ double warp_iscan(double v, int lane) {
   return v;
 }
 
-__device__ __forceinline__ float keogh_term(float x, float U, float L) {
-  const float du = x - U, dl = x - L;
-  return x > U ? du * du : (x < L ? dl * dl : 0.0f);
+// Adds one LB_Keogh term: query sample a (block-centered, scale sq, offset o
+// = query block offset - envelope block offset, both already scaled) against
+// the envelope center/radius cr (scale se).  With U = c + r, L = c - r,
+// max(q - U, 0)^2 + min(q - L, 0)^2 = max(|q - c| - r, 0)^2.
+__device__ __forceinline__ float keogh_acc(float a, float2 cr, float sq, float se, float o,
+                                           float acc) {
+  const float q = fmaf(a, sq, o);
+  const float e = fmaf(cr.x, -se, q);
+  const float d = fmaxf(fmaf(cr.y, -se, fabsf(e)), 0.0f);
+  return fmaf(d, d, acc);
+}
+
+__device__ __forceinline__ float block_offset(const DevSeries& S, unsigned int b, double mu,
+                                              double is) {
+  return (float)((S.cb[b] - mu) * is);
+}
+
+// One direction of LB_Keogh for one pair: the query window starts at qx (mean
+// muq, inverse deviation isq), the envelope's window at ex.  The six end
+// samples enter as max(their terms, kim) (the endpoint bound covers the same
+// cells); the middle samples follow in order in stretches of kKeoghCheck,
+// after each of which the warp compares the running sum with thr.  Each side
+// keeps the scaled offsets of its current and next block, so a stretch that
+// crosses a block boundary selects per lane.  Returns true when the whole
+// bound stays within thr, false as soon as it exceeds it.  Every branch is
+// warp-uniform.
+__device__ bool keogh_within(const DevSeries& S, unsigned int qx, unsigned int ex, double muq,
+                             double mue, double isq, double ise, float kim, float thr, int lane) {
+  // sample indexes stay below 2^31 (n <= INT32_MAX - 4), block ends below 2^32
+  const int m = S.m, kend = m - kBias;
+  const float sq = (float)isq, se = (float)ise;
+  const float* A = S.af + qx;
+  const float2* CR = S.crf + ex;
+  float ends = 0.0f;
+  if (lane < 2 * kBias) {
+    const int k = lane < kBias ? lane : m - 2 * kBias + lane;
+    const float o = block_offset(S, (qx + k) >> kBlkShift, muq, isq) -
+                    block_offset(S, (ex + k) >> kBlkShift, mue, ise);
+    ends = keogh_acc(A[k], CR[k], sq, se, o, 0.0f);
+  }
+  ends = fmaxf(warp_sumf(ends), kim);
+  unsigned int bq = qx >> kBlkShift, be = ex >> kBlkShift;
+  unsigned int nq = (bq + 1) << kBlkShift, ne = (be + 1) << kBlkShift;  // next blocks' first samples
+  float oq = block_offset(S, bq, muq, isq), oq1 = block_offset(S, bq + 1, muq, isq);
+  float oe = block_offset(S, be, mue, ise), oe1 = block_offset(S, be + 1, mue, ise);
+  float acc = 0.0f;
+  for (int k0 = kBias; k0 < kend; k0 += kKeoghCheck) {
+    const int k1 = k0 + kKeoghCheck < kend ? k0 + kKeoghCheck : kend;
+    while (qx + k0 >= nq) {
+      ++bq;
+      nq += 1u << kBlkShift;
+      oq = oq1;
+      oq1 = block_offset(S, bq + 1, muq, isq);
+    }
+    while (ex + k0 >= ne) {
+      ++be;
+      ne += 1u << kBlkShift;
+      oe = oe1;
+      oe1 = block_offset(S, be + 1, mue, ise);
+    }
+    if (qx + k1 <= nq && ex + k1 <= ne) {
+      // both windows stay inside their current block over this stretch
+      const float o = oq - oe;
+#pragma unroll
+      for (int u = 0; u < kKeoghCheck / 32; ++u) {
+        const int k = k0 + u * 32 + lane;
+        if (k < k1) acc = keogh_acc(A[k], CR[k], sq, se, o, acc);
+      }
+    } else {
+      // a stretch is shorter than a block, so it reaches at most the next one
+#pragma unroll
+      for (int u = 0; u < kKeoghCheck / 32; ++u) {
+        const int k = k0 + u * 32 + lane;
+        if (k < k1) {
+          const float o = (qx + k < nq ? oq : oq1) - (ex + k < ne ? oe : oe1);
+          acc = keogh_acc(A[k], CR[k], sq, se, o, acc);
+        }
+      }
+    }
+    if (ends + warp_sumf(acc) > thr) return false;
+  }
+  return true;
 }
 
 // Cuts the survivor bits of one lag into runs; returns how many runs were
@@ -131,17 +215,13 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
                                                          const unsigned int* bits,
                                                          unsigned int total_items, bool masked,
                                                          bool bounds) {
-  __shared__ float offs[kRunWarps][2][kMaxWinBlocks];
   __shared__ unsigned int wbits[kRunWarps][kLbWords];
   __shared__ int2 rlist[kRunWarps][kRunList];
   __shared__ unsigned long long cnt[kNumCounters];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m = S.m, lo = kBias, hi = S.m - 1 - kBias;
-  const int nblk = ((m - 1) >> kBlkShift) + 2;
   for (int x = threadIdx.x; x < kNumCounters; x += blockDim.x) cnt[x] = 0;
   __syncthreads();
-  float* oi = offs[warp][0];
-  float* oj = offs[warp][1];
   unsigned int* wb = wbits[warp];
   int2* rl = rlist[warp];
   for (;;) {
@@ -254,54 +334,20 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
           atomicAdd(&cnt[kPrunedKim], 1ull);
         }
       }
-      // ---- LB_Keogh, one pair at a time ----
-      unsigned int bits = __ballot_sync(0xffffffffu, alive);
-      while (bits) {
-        const int qd = __ffs(bits) - 1;
-        bits &= bits - 1;
-        const int64_t pi = __shfl_sync(0xffffffffu, i, qd);
-        const int64_t pj = __shfl_sync(0xffffffffu, j, qd);
-        const float ends = __shfl_sync(0xffffffffu, kl + kr, qd);
-        const double mui = S.mu[pi], muj = S.mu[pj];
-        const float si = (float)S.isg[pi], sj = (float)S.isg[pj];
-        const int64_t bi = pi >> kBlkShift, bj = pj >> kBlkShift;
-        if (lane < nblk) {
-          oi[lane] = (float)(S.cb[bi + lane] - mui);
-          oj[lane] = (float)(S.cb[bj + lane] - muj);
-        }
-        __syncwarp();
-        float s_e1 = 0, s_m1 = 0, s_e2 = 0, s_m2 = 0;
-        bool dead = false;
-        for (int base = 0; base < m && !dead; base += 256) {
-          const int lim = base + 256 < m ? base + 256 : m;
-          for (int k = base + lane; k < lim; k += 32) {
-            const int64_t xi = pi + k, xj = pj + k;
-            const float ofi = oi[(xi >> kBlkShift) - bi], ofj = oj[(xj >> kBlkShift) - bj];
-            const float qi = (S.af[xi] + ofi) * si, tj = (S.af[xj] + ofj) * sj;
-            const float t1 = keogh_term(qi, (S.Uf[xj] + ofj) * sj, (S.Lf[xj] + ofj) * sj);
-            const float t2 = keogh_term(tj, (S.Uf[xi] + ofi) * si, (S.Lf[xi] + ofi) * si);
-            if (k < kBias || k >= m - kBias) {
-              s_e1 += t1;
-              s_e2 += t2;
-            } else {
-              s_m1 += t1;
-              s_m2 += t2;
-            }
-          }
-          const float lb1 = fmaxf(warp_sumf(s_e1), ends) + warp_sumf(s_m1);
-          const float lb2 = fmaxf(warp_sumf(s_e2), ends) + warp_sumf(s_m2);
-          if (lb1 > thr || lb2 > thr) dead = true;
-        }
-        if (lane == 0) {
-          if (dead) {
-            atomicAdd(&cnt[kPrunedKeogh], 1ull);
+      // ---- survivors go to the LB_Keogh queue, in run order ----
+      const unsigned int bits = __ballot_sync(0xffffffffu, alive);
+      if (bits) {
+        unsigned int base = 0;
+        if (lane == 0) base = atomicAdd(Q.kq_count, (unsigned int)__popc(bits));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (alive) {
+          const unsigned int slot = base + __popc(bits & ((1u << lane) - 1u));
+          if (slot < Q.kq_cap) {
+            Q.kq[slot] = make_int4((int)i, (int)j, __float_as_int(kl + kr), 0);
           } else {
-            const unsigned int slot = atomicAdd(Q.queue_count, 1u);
-            if (slot < Q.queue_cap) Q.queue[slot] = make_int2((int)pi, (int)pj);
-            else atomicOr(S.status, 2);
+            atomicOr(S.status, 2);
           }
         }
-        __syncwarp();
       }
       // a fresh best-so-far tightens the rest of the run
       thr = fminf(thr, prune_threshold_now(Q.bsf2, S.m));
@@ -313,6 +359,51 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
   __syncthreads();
   for (int x = threadIdx.x; x < kNumCounters; x += blockDim.x)
     if (cnt[x]) atomicAdd(&Q.counters[x], cnt[x]);
+}
+
+// LB_Keogh over the queued candidates.  Entries sit in the order the run
+// filter found them, so the kKeoghBatch consecutive pairs a warp takes are
+// mostly neighbours on one diagonal and share L1 lines.  Lanes run over the
+// samples of one pair at a time; the first direction (query i against the
+// envelope of j) decides most pairs, the second runs only when the first
+// stays within the best-so-far.
+__global__ void __launch_bounds__(kKeoghWarps * 32, 5) k_keogh(DevSeries S, DevSearch Q) {
+  __shared__ unsigned long long pruned_block;
+  if (threadIdx.x == 0) pruned_block = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned int total = *Q.kq_count < Q.kq_cap ? *Q.kq_count : Q.kq_cap;
+  unsigned long long pruned = 0;
+  for (;;) {
+    unsigned int idx = 0;
+    if (lane == 0) idx = atomicAdd(Q.kq_next, (unsigned int)kKeoghBatch);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= total) break;
+    const unsigned int end = idx + kKeoghBatch < total ? idx + kKeoghBatch : total;
+    const float thr = prune_threshold_now(Q.bsf2, S.m);
+    for (unsigned int e = idx; e < end; ++e) {
+      const int4 r = Q.kq[e];
+      const float kim = __int_as_float(r.z);
+      bool live = true;
+#pragma unroll 1
+      for (int d = 0; d < 2 && live; ++d) {
+        const unsigned int q = d ? r.y : r.x, t = d ? r.x : r.y;
+        live = keogh_within(S, q, t, S.mu[q], S.mu[t], S.isg[q], S.isg[t], kim, thr, lane);
+      }
+      if (lane == 0) {
+        if (!live) {
+          ++pruned;
+        } else {
+          const unsigned int slot = atomicAdd(Q.queue_count, 1u);
+          if (slot < Q.queue_cap) Q.queue[slot] = make_int2(r.x, r.y);
+          else atomicOr(S.status, 2);
+        }
+      }
+    }
+  }
+  if (lane == 0 && pruned) atomicAdd(&pruned_block, pruned);
+  __syncthreads();
+  if (threadIdx.x == 0 && pruned_block) atomicAdd(&Q.counters[kPrunedKeogh], pruned_block);
 }
 
 // Block means of the series (centers of the FP32 copies).
@@ -340,8 +431,7 @@ __global__ void k_center(DevSeries S, int nb) {
   if (p < S.n) {
     const double c = S.cb[p >> kBlkShift];
     S.af[p] = (float)(S.a[p] - c);
-    S.Uf[p] = (float)(S.U[p] - c);
-    S.Lf[p] = (float)(S.L[p] - c);
+    S.crf[p] = make_float2((float)(0.5 * (S.U[p] + S.L[p]) - c), (float)(0.5 * (S.U[p] - S.L[p])));
   }
   // two padding blocks past the end repeat the last center
   if (p < 2) S.cb[nb + p] = S.cb[nb - 1];
@@ -353,6 +443,13 @@ void launch_center(const DevSeries& S, cudaStream_t st) {
   const int nb = (int)((S.n + (1 << kBlkShift) - 1) >> kBlkShift);
   k_block_mean<<<nb, 256, 0, st>>>(S, nb);
   k_center<<<(unsigned)((S.n + 255) / 256), 256, 0, st>>>(S, nb);
+}
+
+void launch_keogh(const DevSeries& S, const DevSearch& Q, int num_sms, cudaStream_t st) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_keogh, kKeoghWarps * 32, 0);
+  if (per_sm < 1) per_sm = 1;
+  k_keogh<<<num_sms * per_sm, kKeoghWarps * 32, 0, st>>>(S, Q);
 }
 
 void launch_runs(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
