@@ -109,7 +109,7 @@ struct DevSeries {
   double* SME;      // s, sum_T M E
   double* cb;       // (n >> kBlkShift) + 2, block centers
   float* af;        // n, a - cb[block]
-  float2* crf;      // n, ((U + L) / 2 - cb[block], (U - L) / 2): envelope center, radius
+  float2* ulf;      // n, (U - cb[block], L - cb[block])
   int* status;      // device status word (0 ok, else error bits)
 };
 

@@ -66,7 +66,7 @@ enum BufId {
   B_AC, B_DUL, B_QSIG, B_MASK, B_MN, B_MDUL2, B_MDUL, B_SM, B_SME, B_STATUS,
   B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
-  B_MP, B_MPI, B_CB, B_AF, B_CRF, B_BITS, B_LBTILES, B_KQ,
+  B_MP, B_MPI, B_CB, B_AF, B_ULF, B_BITS, B_LBTILES, B_KQ,
   B_COUNT_
 };
 
@@ -209,7 +209,7 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   ENSURE(B_SME, s * 8, S.SME);
   ENSURE(B_CB, ((n >> kBlkShift) + 4) * 8, S.cb);
   ENSURE(B_AF, n * 4, S.af);
-  ENSURE(B_CRF, n * 8, S.crf);
+  ENSURE(B_ULF, n * 8, S.ulf);
   ENSURE(B_STATUS, 4, S.status);
   cudaStream_t st = ctx->stream;
   CUDA_OK(cudaMemsetAsync(S.status, 0, 4, st));

@@ -21,8 +21,8 @@
 // kKeoghCheck samples; most pairs that reach it are pruned within the first
 // few hundred samples of the first direction.  The run's windows overlap, so
 // consecutive pairs re-read the same lines from L1.  It reads FP32 copies of
-// the series and of the envelope as (center, radius), centered per
-// 1024-sample block and normalised per window.  Survivors go to the DTW queue.
+// the series and of the envelope (U, L pairs), centered per 1024-sample
+// block and normalised per window.  Survivors go to the DTW queue.
 #include "../../include/dtwj.h"
 #include "dtwj_dev.cuh"
 
@@ -87,15 +87,21 @@ __device__ __forceinline__ double warp_iscan(double v, int lane) {
   return v;
 }
 
+// max(a, b, c) in one instruction (three-input max.f32, sm_100).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+
 // Adds one LB_Keogh term: query sample a (block-centered, scale sq, offset o
 // = query block offset - envelope block offset, both already scaled) against
-// the envelope center/radius cr (scale se).  With U = c + r, L = c - r,
-// max(q - U, 0)^2 + min(q - L, 0)^2 = max(|q - c| - r, 0)^2.
-__device__ __forceinline__ float keogh_acc(float a, float2 cr, float sq, float se, float o,
+// the block-centered envelope ul = (U, L) (scale se).  With q = a sq + o,
+// max(q - U, 0)^2 + min(q - L, 0)^2 = max(q - U, L - q, 0)^2 since L <= U.
+__device__ __forceinline__ float keogh_acc(float a, float2 ul, float sq, float se, float o,
                                            float acc) {
   const float q = fmaf(a, sq, o);
-  const float e = fmaf(cr.x, -se, q);
-  const float d = fmaxf(fmaf(cr.y, -se, fabsf(e)), 0.0f);
+  const float d = max3f(fmaf(ul.x, -se, q), fmaf(ul.y, se, -q), 0.0f);
   return fmaf(d, d, acc);
 }
 
@@ -104,71 +110,61 @@ __device__ __forceinline__ float block_offset(const DevSeries& S, unsigned int b
   return (float)((S.cb[b] - mu) * is);
 }
 
-// One direction of LB_Keogh for one pair: the query window starts at qx (mean
-// muq, inverse deviation isq), the envelope's window at ex.  The six end
-// samples enter as max(their terms, kim) (the endpoint bound covers the same
-// cells); the middle samples follow in order in stretches of kKeoghCheck,
-// after each of which the warp compares the running sum with thr.  Each side
-// keeps the scaled offsets of its current and next block, so a stretch that
-// crosses a block boundary selects per lane.  Returns true when the whole
-// bound stays within thr, false as soon as it exceeds it.  Every branch is
-// warp-uniform.
-__device__ bool keogh_within(const DevSeries& S, unsigned int qx, unsigned int ex, double muq,
-                             double mue, double isq, double ise, float kim, float thr, int lane) {
-  // sample indexes stay below 2^31 (n <= INT32_MAX - 4), block ends below 2^32
-  const int m = S.m, kend = m - kBias;
-  const float sq = (float)isq, se = (float)ise;
-  const float* A = S.af + qx;
-  const float2* CR = S.crf + ex;
-  float ends = 0.0f;
-  if (lane < 2 * kBias) {
-    const int k = lane < kBias ? lane : m - 2 * kBias + lane;
-    const float o = block_offset(S, (qx + k) >> kBlkShift, muq, isq) -
-                    block_offset(S, (ex + k) >> kBlkShift, mue, ise);
-    ends = keogh_acc(A[k], CR[k], sq, se, o, 0.0f);
-  }
-  ends = fmaxf(warp_sumf(ends), kim);
-  unsigned int bq = qx >> kBlkShift, be = ex >> kBlkShift;
-  unsigned int nq = (bq + 1) << kBlkShift, ne = (be + 1) << kBlkShift;  // next blocks' first samples
-  float oq = block_offset(S, bq, muq, isq), oq1 = block_offset(S, bq + 1, muq, isq);
-  float oe = block_offset(S, be, mue, ise), oe1 = block_offset(S, be + 1, mue, ise);
+// One window of a queued LB_Keogh candidate, prefetched into shared memory.
+struct KeoghSide {
+  double mu, is;     // window mean and 1 / deviation
+  float o0, o1;      // (cb - mu) * is of the window's first block and of the next
+  unsigned int x;    // window start (below 2^31: n <= INT32_MAX - 4)
+  unsigned int pad;
+};
+
+// Scaled offset of block b for window side w: the prefetched ones for its
+// first two blocks, FP64 otherwise (windows longer than a block).
+__device__ __forceinline__ float side_offset(const DevSeries& S, const KeoghSide& w,
+                                             unsigned int b) {
+  const unsigned int b0 = w.x >> kBlkShift;
+  return b == b0 ? w.o0 : (b == b0 + 1 ? w.o1 : block_offset(S, b, w.mu, w.is));
+}
+
+// One direction of LB_Keogh for one pair: query window q against the
+// envelope of window e, over the middle samples [kBias, m - kBias); `ends` is
+// the end samples' share (max of their terms and the endpoint bound).  The
+// samples run in segments over which both windows stay in one block (constant
+// offset), each in stretches of kKeoghCheck after which the warp compares the
+// running sum with thr; a segment's remainder joins the sum unchecked.
+// Returns true when the whole bound stays within thr, false as soon as it
+// exceeds it.  Every branch is warp-uniform.
+__device__ bool keogh_within(const DevSeries& S, const KeoghSide& q, const KeoghSide& e,
+                             float ends, float thr, int lane) {
+  const int kend = S.m - kBias;
+  const unsigned int qx = q.x, ex = e.x;
+  const float sq = (float)q.is, se = (float)e.is;
+  const float* A = S.af + qx + lane;
+  const float2* UL = S.ulf + ex + lane;
+  unsigned int bq = (qx + kBias) >> kBlkShift, be = (ex + kBias) >> kBlkShift;
+  float oq = side_offset(S, q, bq), oe = side_offset(S, e, be);
   float acc = 0.0f;
-  for (int k0 = kBias; k0 < kend; k0 += kKeoghCheck) {
-    const int k1 = k0 + kKeoghCheck < kend ? k0 + kKeoghCheck : kend;
-    while (qx + k0 >= nq) {
-      ++bq;
-      nq += 1u << kBlkShift;
-      oq = oq1;
-      oq1 = block_offset(S, bq + 1, muq, isq);
-    }
-    while (ex + k0 >= ne) {
-      ++be;
-      ne += 1u << kBlkShift;
-      oe = oe1;
-      oe1 = block_offset(S, be + 1, mue, ise);
-    }
-    if (qx + k1 <= nq && ex + k1 <= ne) {
-      // both windows stay inside their current block over this stretch
-      const float o = oq - oe;
+  int k = kBias;
+  for (;;) {
+    // first samples of the next blocks, relative to the window starts
+    const int nq = (int)(((bq + 1) << kBlkShift) - qx), ne = (int)(((be + 1) << kBlkShift) - ex);
+    const int seg = min(kend, min(nq, ne));
+    const float o = oq - oe;
+    for (; k + kKeoghCheck <= seg; k += kKeoghCheck) {
 #pragma unroll
-      for (int u = 0; u < kKeoghCheck / 32; ++u) {
-        const int k = k0 + u * 32 + lane;
-        if (k < k1) acc = keogh_acc(A[k], CR[k], sq, se, o, acc);
-      }
-    } else {
-      // a stretch is shorter than a block, so it reaches at most the next one
-#pragma unroll
-      for (int u = 0; u < kKeoghCheck / 32; ++u) {
-        const int k = k0 + u * 32 + lane;
-        if (k < k1) {
-          const float o = (qx + k < nq ? oq : oq1) - (ex + k < ne ? oe : oe1);
-          acc = keogh_acc(A[k], CR[k], sq, se, o, acc);
-        }
-      }
+      for (int u = 0; u < kKeoghCheck / 32; ++u)
+        acc = keogh_acc(A[k + 32 * u], UL[k + 32 * u], sq, se, o, acc);
+      if (ends + warp_sumf(acc) > thr) return false;
     }
-    if (ends + warp_sumf(acc) > thr) return false;
+#pragma unroll
+    for (int u = 0; u < kKeoghCheck / 32; ++u)
+      if (k + 32 * u + lane < seg) acc = keogh_acc(A[k + 32 * u], UL[k + 32 * u], sq, se, o, acc);
+    k = seg;
+    if (k >= kend) break;
+    if (nq == seg) oq = side_offset(S, q, ++bq);
+    if (ne == seg) oe = side_offset(S, e, ++be);
   }
-  return true;
+  return ends + warp_sumf(acc) <= thr;
 }
 
 // Cuts the survivor bits of one lag into runs; returns how many runs were
@@ -322,13 +318,12 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
         alive = false;
         atomicAdd(&cnt[kPrunedMasked], 1ull);
       }
-      float kl = 0.0f, kr = 0.0f;
+      float kim = 0.0f;
       if (alive) {
         const ZEnds zi = z_ends(S, i), zj = z_ends(S, j);
         double dl, dr;
         kim_bound<double>(zi, zj, m, &dl, &dr);
-        kl = (float)dl;
-        kr = (float)dr;
+        kim = (float)(dl + dr);
         if (dl + dr + lbm * lbm > (double)thr) {
           alive = false;
           atomicAdd(&cnt[kPrunedKim], 1ull);
@@ -343,7 +338,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
         if (alive) {
           const unsigned int slot = base + __popc(bits & ((1u << lane) - 1u));
           if (slot < Q.kq_cap) {
-            Q.kq[slot] = make_int4((int)i, (int)j, __float_as_int(kl + kr), 0);
+            Q.kq[slot] = make_int4((int)i, (int)j, __float_as_int(kim), 0);
           } else {
             atomicOr(S.status, 2);
           }
@@ -363,15 +358,19 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
 
 // LB_Keogh over the queued candidates.  Entries sit in the order the run
 // filter found them, so the kKeoghBatch consecutive pairs a warp takes are
-// mostly neighbours on one diagonal and share L1 lines.  Lanes run over the
-// samples of one pair at a time; the first direction (query i against the
-// envelope of j) decides most pairs, the second runs only when the first
-// stays within the best-so-far.
+// mostly neighbours on one diagonal and share L1 lines.  Lane e prefetches
+// entry e of the batch (indices, endpoint bound, window statistics, block
+// offsets) into shared memory, so the dependent loads are paid once per
+// batch; then the lanes run over the samples of one pair at a time.  The
+// first direction (query i against the envelope of j) decides most pairs,
+// the second runs only when the first stays within the best-so-far.
 __global__ void __launch_bounds__(kKeoghWarps * 32, 5) k_keogh(DevSeries S, DevSearch Q) {
+  __shared__ KeoghSide side[kKeoghWarps][kKeoghBatch][2];
+  __shared__ float endsv[kKeoghWarps][kKeoghBatch][2];
   __shared__ unsigned long long pruned_block;
   if (threadIdx.x == 0) pruned_block = 0;
   __syncthreads();
-  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned int total = *Q.kq_count < Q.kq_cap ? *Q.kq_count : Q.kq_cap;
   unsigned long long pruned = 0;
   for (;;) {
@@ -379,23 +378,48 @@ __global__ void __launch_bounds__(kKeoghWarps * 32, 5) k_keogh(DevSeries S, DevS
     if (lane == 0) idx = atomicAdd(Q.kq_next, (unsigned int)kKeoghBatch);
     idx = __shfl_sync(0xffffffffu, idx, 0);
     if (idx >= total) break;
-    const unsigned int end = idx + kKeoghBatch < total ? idx + kKeoghBatch : total;
-    const float thr = prune_threshold_now(Q.bsf2, S.m);
-    for (unsigned int e = idx; e < end; ++e) {
-      const int4 r = Q.kq[e];
-      const float kim = __int_as_float(r.z);
-      bool live = true;
-#pragma unroll 1
-      for (int d = 0; d < 2 && live; ++d) {
-        const unsigned int q = d ? r.y : r.x, t = d ? r.x : r.y;
-        live = keogh_within(S, q, t, S.mu[q], S.mu[t], S.isg[q], S.isg[t], kim, thr, lane);
+    const int cnt = total - idx < (unsigned int)kKeoghBatch ? (int)(total - idx) : kKeoghBatch;
+    __syncwarp();  // the previous batch is no longer read
+    if (lane < 2 * cnt) {
+      // lane (e, d): window d of entry e, and the end samples of direction d
+      // (query = window d, envelope = the other window) in FP64
+      const int e = lane >> 1, d = lane & 1;
+      const int4 r = Q.kq[idx + e];
+      const unsigned int xe = (unsigned int)(d ? r.x : r.y);
+      KeoghSide w;
+      w.x = (unsigned int)(d ? r.y : r.x);
+      w.mu = S.mu[w.x];
+      w.is = S.isg[w.x];
+      const unsigned int b0 = w.x >> kBlkShift;
+      w.o0 = block_offset(S, b0, w.mu, w.is);
+      w.o1 = block_offset(S, b0 + 1, w.mu, w.is);
+      w.pad = 0;
+      side[warp][e][d] = w;
+      const double me = S.mu[xe], ie = S.isg[xe];
+      double t = 0.0;
+#pragma unroll
+      for (int c = 0; c < 2 * kBias; ++c) {
+        const int k = c < kBias ? c : S.m - 2 * kBias + c;
+        const double z = (S.a[w.x + k] - w.mu) * w.is;
+        const double u = (S.U[xe + k] - me) * ie, l = (S.L[xe + k] - me) * ie;
+        const double dd = fmax(fmax(z - u, l - z), 0.0);
+        t = fma(dd, dd, t);
       }
+      endsv[warp][e][d] = (float)fmax((double)__int_as_float(r.z), t);
+    }
+    __syncwarp();
+    const float thr = prune_threshold_now(Q.bsf2, S.m);
+    for (int e = 0; e < cnt; ++e) {
+      const KeoghSide& wi = side[warp][e][0];
+      const KeoghSide& wj = side[warp][e][1];
+      bool live = keogh_within(S, wi, wj, endsv[warp][e][0], thr, lane);
+      if (live) live = keogh_within(S, wj, wi, endsv[warp][e][1], thr, lane);
       if (lane == 0) {
         if (!live) {
           ++pruned;
         } else {
           const unsigned int slot = atomicAdd(Q.queue_count, 1u);
-          if (slot < Q.queue_cap) Q.queue[slot] = make_int2(r.x, r.y);
+          if (slot < Q.queue_cap) Q.queue[slot] = make_int2((int)wi.x, (int)wj.x);
           else atomicOr(S.status, 2);
         }
       }
@@ -431,7 +455,7 @@ __global__ void k_center(DevSeries S, int nb) {
   if (p < S.n) {
     const double c = S.cb[p >> kBlkShift];
     S.af[p] = (float)(S.a[p] - c);
-    S.crf[p] = make_float2((float)(0.5 * (S.U[p] + S.L[p]) - c), (float)(0.5 * (S.U[p] - S.L[p])));
+    S.ulf[p] = make_float2((float)(S.U[p] - c), (float)(S.L[p] - c));
   }
   // two padding blocks past the end repeat the last center
   if (p < 2) S.cb[nb + p] = S.cb[nb - 1];
