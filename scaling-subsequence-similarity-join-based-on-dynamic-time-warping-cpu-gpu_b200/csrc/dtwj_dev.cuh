@@ -38,12 +38,16 @@ constexpr double kPadQd = 1e150;
 constexpr double kPadTd = -1e150;
 
 // Lag-block x row-block of the diagonal sweep: pairs (i, i + L) for
-// L in [L0, L0 + kTileLags) and i in [i0, i0 + rows).
+// L in [L0, L0 + kLbLags) and i in [i0, i0 + rows), all windows below send.
+// Indices are global: in a batch the series sit back to back and a tile
+// belongs to one of them.
 struct Tile {
   int32_t L0;
   int32_t i0;
   int32_t rows;
-  int32_t order;  // position in the queue order (learned or plain)
+  int32_t order;   // position in the queue order (learned or plain)
+  int32_t send;    // end of the series' windows (global window index)
+  int32_t series;  // series of the batch (0 for a single join)
 };
 constexpr int kTileLags = 128;
 // Diagonal-sweep tiles: 128 threads x kLbPerThread lags x kLbRows rows, one
@@ -77,15 +81,18 @@ enum Counter {
 struct Candidate {
   int32_t i, j;
   float d2;
-  int32_t pad;
+  int32_t series;
 };
 
 // All device arrays of one prepared series.
 struct DevSeries {
-  const double* a;  // n, the series
+  const double* a;  // n, the series (a batch: all series back to back)
   int64_t n;
   int64_t s;        // n - m + 1
   int m, w;
+  const int* sid;   // n, series of each sample (nullptr for a single series)
+  const int64_t* sbeg;  // series + 1 sample offsets (nullptr for a single series)
+  int nseries;
   double* mu;       // s, window mean
   double* sig;      // s, window population std (1 for flat windows)
   double* isg;      // s, 1/sig (0 for flat windows)
@@ -115,7 +122,7 @@ struct DevSeries {
 
 // Global search state of one join.
 struct DevSearch {
-  unsigned int* bsf2;           // float bits of the best squared DTW so far
+  unsigned int* bsf2;           // per series: float bits of the best squared DTW so far
   unsigned long long* counters; // kNumCounters
   Candidate* cand;              // candidate list
   unsigned int* cand_count;
@@ -172,6 +179,8 @@ bool choose_band(int w, BandShape* out);
 
 // ---- launches (all on `stream`) ----
 void launch_check_finite(const double* a, int64_t n, int* status, cudaStream_t st);
+// sid[p] = series of sample p for a batch with series offsets sbeg[0..nseries].
+void launch_series_ids(const int64_t* sbeg, int nseries, int* sid, int64_t n, cudaStream_t st);
 void launch_prep(const DevSeries& S, cudaStream_t st);
 void launch_rowterms(const DevSeries& S, bool masked, cudaStream_t st);
 // Largest CDF length the mask can need: max |z| <= sqrt(m - 1).
@@ -186,12 +195,21 @@ void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
                         const unsigned long long* lo, double* mp, int64_t* mpi,
                         cudaStream_t st);
 void launch_reverse(const double* a, int64_t n, double* out, cudaStream_t st);
+// kSeeds seeds per series into seeds[series * kSeeds ...] (unused slots hold
+// (-1, -1)), their counts into nseeds[series] and the initial best-so-far
+// into bsf2[series].
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
                         unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st);
+// Series of a sample (0 for a single series).
+__device__ __forceinline__ int series_of(const DevSeries& S, int64_t x) {
+  return S.sid ? S.sid[x] : 0;
+}
 // Fast diagonal bound over LB tiles [tile_begin, tile_end); survivors leave
 // as bits, [tile][lag][word].  enumerate_all: no pruning (bounds off).
+// Persistent: CTAs take tiles from the work counter *next (zero at launch).
 void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
-               int tile_end, unsigned int* bits, bool enumerate_all, cudaStream_t st);
+               int tile_end, unsigned int* bits, bool enumerate_all, unsigned int* next,
+               int num_sms, cudaStream_t st);
 size_t lb_smem_bytes();
 // Run filter over the survivor bits of LB tiles [tile_begin, tile_end):
 // masked bound, endpoint bound and LB_Keogh for every pair of every run of
@@ -207,8 +225,12 @@ void launch_keogh(const DevSeries& S, const DevSearch& Q, int num_sms, cudaStrea
 void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
                   const unsigned int* npairs, bool bounds, BandShape band, int num_sms,
                   cudaStream_t st);
+// FP64 re-verification of the candidates, then per series the lexicographic
+// minimum (d2, i, j): best_d2[series] (FP64 squared distance, +inf if none),
+// best_ij[series] = i << 32 | j, best_f32[series] = the search's FP32 d2.
 void launch_verify(const DevSeries& S, const DevSearch& Q, BandShape band, double* out_d2,
-                   double* best_d2, int* best_idx, cudaStream_t st);
+                   unsigned long long* best_d2, unsigned long long* best_ij, float* best_f32,
+                   cudaStream_t st);
 void launch_pair_dtw(const DevSeries& S, const int2* pairs, int count, bool precise,
                      BandShape band, double* out_d2, cudaStream_t st);
 

@@ -15,6 +15,7 @@
 #include "../../include/dtwj.h"
 #include "dtwj_dev.cuh"
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -55,7 +56,8 @@ struct dtwj_ctx {
   std::vector<Buf> bufs;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<Tile> lbtiles_host;    // kLbLags-lag tiles of the diagonal sweep
-  int64_t lbtiles_n = -1, lbtiles_m = -1;
+  int64_t lbtiles_n = -1, lbtiles_m = -1;  // single-series shape the tiles were built for
+  std::vector<unsigned int> host_u32;      // staging of small host -> device copies
   std::vector<cudaEvent_t> pool;  // events for per-phase device times
 };
 
@@ -66,7 +68,8 @@ enum BufId {
   B_AC, B_DUL, B_QSIG, B_MASK, B_MN, B_MDUL2, B_MDUL, B_SM, B_SME, B_STATUS,
   B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
-  B_MP, B_MPI, B_CB, B_AF, B_ULF, B_BITS, B_LBTILES, B_KQ,
+  B_MP, B_MPI, B_CB, B_AF, B_ULF, B_BITS, B_LBTILES, B_KQ, B_SBEG, B_SID, B_SEEDBSF,
+  B_BEST_IJ, B_BEST_F32,
   B_COUNT_
 };
 
@@ -155,29 +158,38 @@ int check_args(const void* x, int64_t n, int32_t m, int32_t w) {
   return DTWJ_OK;
 }
 
-void build_lb_tiles(dtwj_ctx* ctx, int64_t n, int m) {
-  if (ctx->lbtiles_n == n && ctx->lbtiles_m == m) return;
-  const int64_t s = n - m + 1;
+// Tiles of the profile and the diagonal sweep (kLbLags lags x kLbRows rows)
+// for every series; a single series keeps its tiles across calls.
+void build_lb_tiles(dtwj_ctx* ctx, int64_t n, int m, const int64_t* sbeg, int nseries) {
+  if (!sbeg && ctx->lbtiles_n == n && ctx->lbtiles_m == m) return;
   ctx->lbtiles_host.clear();
   int32_t order = 0;
-  for (int64_t L0 = m; L0 <= s - 1; L0 += kLbLags) {
-    const int64_t rows_total = s - L0;
-    for (int64_t i0 = 0; i0 < rows_total; i0 += kLbRows) {
-      Tile t;
-      t.L0 = (int32_t)L0;
-      t.i0 = (int32_t)i0;
-      t.rows = (int32_t)(rows_total - i0 < kLbRows ? rows_total - i0 : kLbRows);
-      t.order = order++;
-      ctx->lbtiles_host.push_back(t);
+  for (int r = 0; r < nseries; ++r) {
+    const int64_t wb = sbeg ? sbeg[r] : 0;
+    const int64_t s = (sbeg ? sbeg[r + 1] - sbeg[r] : n) - m + 1;
+    for (int64_t L0 = m; L0 <= s - 1; L0 += kLbLags) {
+      const int64_t rows_total = s - L0;
+      for (int64_t i0 = 0; i0 < rows_total; i0 += kLbRows) {
+        Tile t;
+        t.L0 = (int32_t)L0;
+        t.i0 = (int32_t)(wb + i0);
+        t.rows = (int32_t)(rows_total - i0 < kLbRows ? rows_total - i0 : kLbRows);
+        t.order = order++;
+        t.send = (int32_t)(wb + s);
+        t.series = r;
+        ctx->lbtiles_host.push_back(t);
+      }
     }
   }
-  ctx->lbtiles_n = n;
-  ctx->lbtiles_m = m;
+  ctx->lbtiles_n = sbeg ? -1 : n;
+  ctx->lbtiles_m = sbeg ? -1 : m;
 }
 
-// Allocates and prepares every per-series array; returns the DevSeries.
+// Allocates and prepares every per-series array; returns the DevSeries.  A
+// batch (sbeg != nullptr) holds nseries series back to back in x_dev, series
+// r on samples [sbeg[r], sbeg[r + 1]).
 int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool masked,
-            DevSeries* out, Phases* ph = nullptr) {
+            const int64_t* sbeg_host, int nseries, DevSeries* out, Phases* ph = nullptr) {
   const int64_t s = n - m + 1;
   DevSeries S;
   memset(&S, 0, sizeof S);
@@ -186,6 +198,18 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   S.s = s;
   S.m = m;
   S.w = w;
+  S.nseries = nseries;
+  if (sbeg_host) {
+    int64_t* sbeg;
+    int* sid;
+    ENSURE(B_SBEG, (size_t)(nseries + 1) * 8, sbeg);
+    ENSURE(B_SID, (size_t)n * 4, sid);
+    CUDA_OK(cudaMemcpyAsync(sbeg, sbeg_host, (size_t)(nseries + 1) * 8, cudaMemcpyHostToDevice,
+                            ctx->stream));
+    launch_series_ids(sbeg, nseries, sid, n, ctx->stream);
+    S.sbeg = sbeg;
+    S.sid = sid;
+  }
   ENSURE(B_MU, s * 8, S.mu);
   ENSURE(B_SIG, s * 8, S.sig);
   ENSURE(B_ISG, s * 8, S.isg);
@@ -244,31 +268,35 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
 
 int effective_band(int m, int w) { return w > m - 1 ? m - 1 : w; }
 
-int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_t w_in,
-                uint32_t flags, dtwj_result* out, double t_upload) {
+// Joins one series (sbeg == nullptr, nseries == 1) or a batch of nseries
+// series of one (m, w) stored back to back (series r on samples
+// [sbeg[r], sbeg[r + 1])); outs[r] receives series r's top-1 pair with
+// indices relative to its own first sample.
+int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg, int nseries,
+             int32_t m, int32_t w_in, uint32_t flags, dtwj_result* outs, double t_upload) {
   Timer wall;
   const int w = effective_band(m, w_in);
   BandShape band;
   if (!choose_band(w, &band)) return DTWJ_ERR_BAND;
   if (flags & DTWJ_F_LEARNED) return DTWJ_ERR_NOMODEL;
-  const bool masked = !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
+  // the masked bound's CDF tables are per series; batches go without it
+  const bool masked = !sbeg && !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
   const bool verbose = flags & DTWJ_F_VERBOSE;
   cudaStream_t st = ctx->stream;
   Phases ph(ctx, (flags & DTWJ_F_PROFILE) != 0);
   CUDA_OK(cudaEventRecord(ctx->ev0, st));
 
   DevSeries S;
-  int rc = prepare(ctx, x_dev, n, m, w, masked, &S, &ph);
+  int rc = prepare(ctx, x_dev, n, m, w, masked, sbeg, nseries, &S, &ph);
   if (rc) return rc;
-  const int64_t s = S.s;
 
-  // tiles of the profile and the diagonal sweep (kLbLags lags x kLbRows rows)
-  build_lb_tiles(ctx, n, m);
+  build_lb_tiles(ctx, n, m, sbeg, nseries);
   const int nlb = (int)ctx->lbtiles_host.size();
   Tile* lbtiles;
-  ENSURE(B_LBTILES, (size_t)nlb * sizeof(Tile), lbtiles);
-  CUDA_OK(cudaMemcpyAsync(lbtiles, ctx->lbtiles_host.data(), (size_t)nlb * sizeof(Tile),
-                          cudaMemcpyHostToDevice, st));
+  ENSURE(B_LBTILES, (size_t)(nlb > 0 ? nlb : 1) * sizeof(Tile), lbtiles);
+  if (nlb > 0)
+    CUDA_OK(cudaMemcpyAsync(lbtiles, ctx->lbtiles_host.data(), (size_t)nlb * sizeof(Tile),
+                            cudaMemcpyHostToDevice, st));
 
   // search state
   DevSearch Q;
@@ -289,45 +317,48 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   Q.run_next = qc + 3;
   Q.kq_count = qc + 4;
   Q.kq_next = qc + 5;
+  unsigned int* lb_next = qc + 6;
   Q.queue_cap = qcap;
   Q.kq_cap = qcap * 2;
   Q.runs = nullptr;
   Q.run_cap = 0;
-  ENSURE(B_BSF2, 4, Q.bsf2);
+  ENSURE(B_BSF2, (size_t)nseries * 4, Q.bsf2);
   ENSURE(B_COUNTERS, kNumCounters * 8, Q.counters);
   ENSURE(B_CAND, (size_t)kCandCap * sizeof(Candidate), Q.cand);
   ENSURE(B_CCOUNT, 4, Q.cand_count);
   Q.cand_cap = kCandCap;
   CUDA_OK(cudaMemsetAsync(Q.counters, 0, kNumCounters * 8, st));
   CUDA_OK(cudaMemsetAsync(Q.cand_count, 0, 4, st));
-  const unsigned int inf_bits = 0x7f800000u;
-  CUDA_OK(cudaMemcpyAsync(Q.bsf2, &inf_bits, 4, cudaMemcpyHostToDevice, st));
+  ctx->host_u32.assign((size_t)nseries + 1, 0x7f800000u);  // +inf per series
+  CUDA_OK(cudaMemcpyAsync(Q.bsf2, ctx->host_u32.data(), (size_t)nseries * 4,
+                          cudaMemcpyHostToDevice, st));
+  unsigned int* seed_bsf;
+  ENSURE(B_SEEDBSF, (size_t)nseries * 4, seed_bsf);
 
   // ---- ED profile seeds ----
-  float seed_bsf2 = INFINITY;
-  unsigned int* seed_slot = nullptr;
-  if (!(flags & DTWJ_F_NO_SEED)) {
+  if (!(flags & DTWJ_F_NO_SEED) && nlb > 0) {
     unsigned long long* keys;
-    ENSURE(B_KEYS_UP, s * 8, keys);
+    ENSURE(B_KEYS_UP, S.s * 8, keys);
     ph.begin();
     launch_mp(S, lbtiles, nlb, keys, st);
     ph.end(DTWJ_PHASE_PROFILE, 2);
     int2* seeds;
-    unsigned int* nseeds;
-    ENSURE(B_SEEDS, kSeeds * sizeof(int2), seeds);
-    ENSURE(B_NSEEDS, 16, nseeds);
-    CUDA_OK(cudaMemsetAsync(nseeds, 0, 16, st));
+    unsigned int* nseeds;  // [nseries] counts, total slots, work counter
+    ENSURE(B_SEEDS, (size_t)nseries * kSeeds * sizeof(int2), seeds);
+    ENSURE(B_NSEEDS, ((size_t)nseries + 2) * 4, nseeds);
+    ctx->host_u32[0] = (unsigned int)(nseries * kSeeds);
+    CUDA_OK(cudaMemcpyAsync(nseeds + nseries, ctx->host_u32.data(), 4, cudaMemcpyHostToDevice,
+                            st));
+    CUDA_OK(cudaMemsetAsync(nseeds + nseries + 1, 0, 4, st));
     ph.begin();
     launch_seed_select(S, keys, seeds, nseeds, Q.bsf2, st);
-    CUDA_OK(cudaMemsetAsync(nseeds + 1, 0, 4, st));
     DevSearch Qs = Q;
-    Qs.queue_next = nseeds + 1;
-    Qs.queue_cap = kSeeds;
-    launch_pairs(S, Qs, seeds, nseeds, false, band, ctx->num_sms, st);
+    Qs.queue_next = nseeds + nseries + 1;
+    Qs.queue_cap = (unsigned int)(nseries * kSeeds);
+    launch_pairs(S, Qs, seeds, nseeds + nseries, false, band, ctx->num_sms, st);
     ph.end(DTWJ_PHASE_SEEDS, 2);
-    CUDA_OK(cudaMemcpyAsync(nseeds + 2, Q.bsf2, 4, cudaMemcpyDeviceToDevice, st));
-    seed_slot = nseeds + 2;
   }
+  CUDA_OK(cudaMemcpyAsync(seed_bsf, Q.bsf2, (size_t)nseries * 4, cudaMemcpyDeviceToDevice, st));
 
   // ---- diagonal sweep in chunks of LB tiles ----
   const bool enumerate_all = flags & DTWJ_F_NO_DIAG;
@@ -335,13 +366,13 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
   int chunk = kLbChunkTiles;
   if (enumerate_all) chunk = (int)((double)qcap / tile_pairs) > 0 ? (int)((double)qcap / tile_pairs) : 1;
   unsigned int* bits;
-  ENSURE(B_BITS, (size_t)(chunk < nlb ? chunk : nlb) * kLbLags * kLbWords * 4, bits);
+  ENSURE(B_BITS, (size_t)(chunk < nlb ? chunk : (nlb > 0 ? nlb : 1)) * kLbLags * kLbWords * 4, bits);
   for (int attempt = 0;; ++attempt) {
     for (int t0 = 0; t0 < nlb; t0 += chunk) {
       const int t1 = t0 + chunk < nlb ? t0 + chunk : nlb;
       CUDA_OK(cudaMemsetAsync(qc, 0, 32, st));
       ph.begin();
-      launch_lb(S, Q, lbtiles, t0, t1, bits, enumerate_all, st);
+      launch_lb(S, Q, lbtiles, t0, t1, bits, enumerate_all, lb_next, ctx->num_sms, st);
       ph.end(DTWJ_PHASE_DIAG, 1);
       ph.begin();
       launch_runs(S, Q, lbtiles, t0, t1, bits, masked, !enumerate_all, ctx->num_sms, st);
@@ -367,71 +398,83 @@ int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_
     CUDA_OK(cudaMemsetAsync(Q.counters, 0, kNumCounters * 8, st));
   }
 
-  // ---- FP64 verification of the candidates ----
+  // ---- FP64 verification of the candidates, per-series minimum ----
   double* vd2;
   ENSURE(B_VERIFY, (size_t)kCandCap * 8, vd2);
-  double* best;
-  ENSURE(B_BEST, 16, best);
-  int* best_idx = reinterpret_cast<int*>(best + 1);
+  unsigned long long *best_d2, *best_ij;
+  float* best_f32;
+  ENSURE(B_BEST, (size_t)nseries * 8, best_d2);
+  ENSURE(B_BEST_IJ, (size_t)nseries * 8, best_ij);
+  ENSURE(B_BEST_F32, (size_t)nseries * 4, best_f32);
   ph.begin();
-  launch_verify(S, Q, band, vd2, best, best_idx, st);
-  ph.end(DTWJ_PHASE_VERIFY, 2);
+  launch_verify(S, Q, band, vd2, best_d2, best_ij, best_f32, st);
+  ph.end(DTWJ_PHASE_VERIFY, 4);
   CUDA_OK(cudaEventRecord(ctx->ev1, st));
 
-  double best_h[2];
+  std::vector<unsigned long long> d2_h(nseries), ij_h(nseries);
+  std::vector<unsigned int> f32_h(nseries), seed_h(nseries);
   unsigned long long cnt_h[kNumCounters];
-  unsigned int cand_h = 0, bsf_h = 0;
+  unsigned int cand_h = 0;
   int status_h = 0;
-  CUDA_OK(cudaMemcpyAsync(best_h, best, 16, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(d2_h.data(), best_d2, (size_t)nseries * 8, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(ij_h.data(), best_ij, (size_t)nseries * 8, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(f32_h.data(), best_f32, (size_t)nseries * 4, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(seed_h.data(), seed_bsf, (size_t)nseries * 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaMemcpyAsync(cnt_h, Q.counters, sizeof cnt_h, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaMemcpyAsync(&cand_h, Q.cand_count, 4, cudaMemcpyDeviceToHost, st));
-  CUDA_OK(cudaMemcpyAsync(&bsf_h, Q.bsf2, 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaMemcpyAsync(&status_h, S.status, 4, cudaMemcpyDeviceToHost, st));
-  if (seed_slot) CUDA_OK(cudaMemcpyAsync(&seed_bsf2, seed_slot, 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));
   if (status_h & 2) return DTWJ_ERR_OVERFLOW;
   if (cand_h > kCandCap) return DTWJ_ERR_OVERFLOW;
-  int bidx;
-  memcpy(&bidx, &best_h[1], 4);
-  Candidate bc;
-  memset(&bc, 0, sizeof bc);
-  if (bidx >= 0) {
-    CUDA_OK(cudaMemcpy(&bc, Q.cand + bidx, sizeof bc, cudaMemcpyDeviceToHost));
-  }
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
 
-  memset(out, 0, sizeof *out);
-  out->n = n;
-  out->m = m;
-  out->w = w_in;
-  if (bidx >= 0) {
-    out->i = bc.i;
-    out->j = bc.j;
-    out->dist = std::sqrt(best_h[0]);
-    out->dist_fp32 = std::sqrt((double)bc.d2);
-  } else {
-    out->i = out->j = -1;
-    out->dist = out->dist_fp32 = INFINITY;
+  for (int r = 0; r < nseries; ++r) {
+    dtwj_result* out = &outs[r];
+    memset(out, 0, sizeof *out);
+    const int64_t base = sbeg ? sbeg[r] : 0;
+    out->n = sbeg ? sbeg[r + 1] - sbeg[r] : n;
+    out->m = m;
+    out->w = w_in;
+    if (d2_h[r] != ~0ull) {
+      double d2;
+      memcpy(&d2, &d2_h[r], 8);
+      float f2;
+      memcpy(&f2, &f32_h[r], 4);
+      out->i = (int64_t)(ij_h[r] >> 32) - base;
+      out->j = (int64_t)(ij_h[r] & 0xffffffffull) - base;
+      out->dist = std::sqrt(d2);
+      out->dist_fp32 = std::sqrt((double)f2);
+    } else {
+      out->i = out->j = -1;
+      out->dist = out->dist_fp32 = INFINITY;
+    }
+    float sb;
+    memcpy(&sb, &seed_h[r], 4);
+    out->seed_bsf = std::sqrt((double)sb);
+    out->seconds_join = ms / 1000.0;
+    out->seconds_total = wall.seconds() + t_upload;
+    if (!sbeg) {  // the counters are the whole call's: per series only for a single join
+      out->pairs = cnt_h[kPairs];
+      out->pruned_fast = cnt_h[kPrunedFast];
+      out->pruned_kim = cnt_h[kPrunedKim];
+      out->pruned_masked = cnt_h[kPrunedMasked];
+      out->pruned_keogh = cnt_h[kPrunedKeogh];
+      out->dtw_calls = cnt_h[kDtwCalls];
+      out->dtw_abandoned = cnt_h[kDtwAbandoned];
+      out->dtw_cells = cnt_h[kDtwCells];
+      out->candidates = cand_h;
+      ph.collect(out);
+    }
   }
-  out->seed_bsf = std::sqrt((double)seed_bsf2);
-  out->pairs = cnt_h[kPairs];
-  out->pruned_fast = cnt_h[kPrunedFast];
-  out->pruned_kim = cnt_h[kPrunedKim];
-  out->pruned_masked = cnt_h[kPrunedMasked];
-  out->pruned_keogh = cnt_h[kPrunedKeogh];
-  out->dtw_calls = cnt_h[kDtwCalls];
-  out->dtw_abandoned = cnt_h[kDtwAbandoned];
-  out->dtw_cells = cnt_h[kDtwCells];
-  out->candidates = cand_h;
-  out->seconds_join = ms / 1000.0;
-  out->seconds_total = wall.seconds() + t_upload;
-  ph.collect(out);
-  (void)bsf_h;
   if (verbose)
-    fprintf(stderr, "dtwj: join (%lld, %lld) %.6f, %.3fs device\n", (long long)out->i,
-            (long long)out->j, out->dist, out->seconds_join);
+    fprintf(stderr, "dtwj: %d series, %.3fs device, %u candidates\n", nseries, ms / 1000.0, cand_h);
   return DTWJ_OK;
+}
+
+int join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t m, int32_t w_in,
+                uint32_t flags, dtwj_result* out, double t_upload) {
+  return run_join(ctx, x_dev, n, nullptr, 1, m, w_in, flags, out, t_upload);
 }
 
 int upload(dtwj_ctx* ctx, const double* x, int64_t n, double** dev) {
@@ -528,11 +571,51 @@ int dtwj_join(const double* x, int64_t n, int32_t m, int32_t w, uint32_t flags,
 int dtwj_join_batch(const double* const* xs, const int64_t* ns, const int32_t* ms,
                     const int32_t* ws, int32_t count, uint32_t flags, dtwj_result* outs) {
   if (!xs || !ns || !ms || !ws || !outs || count < 0) return DTWJ_ERR_ARG;
+  int rc = DTWJ_OK;
+  for (int32_t k = 0; k < count && rc == DTWJ_OK; ++k) rc = check_args(xs[k], ns[k], ms[k], ws[k]);
+  if (rc || count == 0) return rc;
+  // series of one (m, effective band) are joined together, back to back
+  std::vector<int32_t> order(count);
+  for (int32_t k = 0; k < count; ++k) order[k] = k;
+  auto key = [&](int32_t k) {
+    return ((int64_t)ms[k] << 32) | (uint32_t)effective_band(ms[k], ws[k]);
+  };
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int32_t a, int32_t b) { return key(a) < key(b); });
   dtwj_ctx* ctx = nullptr;
-  int rc = dtwj_ctx_create(0, &ctx);
+  rc = dtwj_ctx_create(0, &ctx);
   if (rc) return rc;
-  for (int32_t k = 0; k < count && rc == DTWJ_OK; ++k)
-    rc = dtwj_ctx_join(ctx, xs[k], ns[k], ms[k], ws[k], flags, &outs[k]);
+  std::vector<double> cat;
+  std::vector<int64_t> sbeg;
+  std::vector<dtwj_result> res;
+  for (int32_t g0 = 0; g0 < count && rc == DTWJ_OK;) {
+    int32_t g1 = g0;
+    while (g1 < count && key(order[g1]) == key(order[g0])) ++g1;
+    const int nser = g1 - g0;
+    sbeg.assign(1, 0);
+    for (int32_t q = g0; q < g1; ++q) sbeg.push_back(sbeg.back() + ns[order[q]]);
+    const int64_t total = sbeg.back();
+    if (total > (int64_t)INT32_MAX - 4) {
+      rc = DTWJ_ERR_ARG;
+      break;
+    }
+    cat.resize((size_t)total);
+    for (int32_t q = g0; q < g1; ++q)
+      memcpy(cat.data() + sbeg[q - g0], xs[order[q]], (size_t)ns[order[q]] * 8);
+    double* dev = nullptr;
+    Timer t;
+    rc = upload(ctx, cat.data(), total, &dev);
+    if (rc) break;
+    res.resize((size_t)nser);
+    rc = run_join(ctx, dev, total, sbeg.data(), nser, ms[order[g0]], ws[order[g0]], flags,
+                  res.data(), 0.0);
+    for (int q = 0; q < nser && rc == DTWJ_OK; ++q) {
+      res[q].w = ws[order[g0 + q]];
+      res[q].seconds_total = t.seconds();
+      outs[order[g0 + q]] = res[q];
+    }
+    g0 = g1;
+  }
   dtwj_ctx_destroy(ctx);
   return rc;
 }
@@ -565,9 +648,9 @@ int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64
       break;
     }
     DevSeries S, R;
-    if ((rc = prepare(ctx, dev, n, m, 0, false, &S))) break;
-    if ((rc = prepare(rev, rdev, n, m, 0, false, &R))) break;
-    build_lb_tiles(ctx, n, m);
+    if ((rc = prepare(ctx, dev, n, m, 0, false, nullptr, 1, &S))) break;
+    if ((rc = prepare(rev, rdev, n, m, 0, false, nullptr, 1, &R))) break;
+    build_lb_tiles(ctx, n, m, nullptr, 1);
     const int nlb = (int)ctx->lbtiles_host.size();
     if ((rc = ensure(ctx, B_LBTILES, (size_t)nlb * sizeof(Tile), &p))) break;
     Tile* tiles = (Tile*)p;
@@ -622,7 +705,7 @@ int dtwj_pair_dtw(const double* x, int64_t n, int32_t m, int32_t w, const int64_
     double* dev = nullptr;
     if ((rc = upload(ctx, x, n, &dev))) break;
     DevSeries S;
-    if ((rc = prepare(ctx, dev, n, m, we, false, &S))) break;
+    if ((rc = prepare(ctx, dev, n, m, we, false, nullptr, 1, &S))) break;
     void* p;
     if ((rc = ensure(ctx, B_PAIRS, (size_t)count * sizeof(int2), &p))) break;
     int2* dp = (int2*)p;

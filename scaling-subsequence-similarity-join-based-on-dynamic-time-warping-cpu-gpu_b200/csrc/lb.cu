@@ -40,25 +40,28 @@ struct LbShared {
   double r1[kStage], r2[kStage], r3[kStage], r4[kStage], rs[kStage], rg[kStage];
 };
 
+// G of window x; flat windows (A = 1e300) get +1e300 whatever the
+// best-so-far, so every pair with a flat window is pruned, also while the
+// best-so-far is still +inf or with the bounds off.
 __device__ __forceinline__ double g_of(const DevSeries& S, int64_t x, double twoB) {
+  const double A = S.A[x];
+  if (A >= 1e299) return 1e300;
   const double t = twoB + S.DUL[x];
-  return S.qsig[x] * fma(-t, t, S.A[x]);
+  return S.qsig[x] * fma(-t, t, A);
 }
 
-__global__ void __launch_bounds__(kLbThreads, 2) k_lb(DevSeries S, DevSearch Q,
-                                                      const Tile* tiles, unsigned int* bits,
-                                                      bool enumerate_all) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  LbShared& sh = *reinterpret_cast<LbShared*>(smraw);
-  const Tile T = tiles[blockIdx.x];
-  const int64_t s = S.s;
+// One tile of the sweep (the body of the persistent k_lb below).
+__device__ __forceinline__ void lb_tile(const DevSeries& S, const DevSearch& Q, const Tile& T,
+                                        unsigned int* out, bool enumerate_all, LbShared& sh,
+                                        unsigned int& npairs, unsigned int& nfast) {
+  const int64_t s = T.send;  // windows of the tile's series end here
   const int m = S.m;
-  const int t = threadIdx.x, lane = t & 31;
+  const int t = threadIdx.x;
   const int64_t L0 = T.L0, i0 = T.i0;
   const int64_t Lt = L0 + (int64_t)t * kLbPerThread;  // this thread's first lag
-  unsigned int* out = bits + (size_t)blockIdx.x * kLbLags * kLbWords;
 
-  const float b2 = enumerate_all ? __int_as_float(0x7f800000) : prune_threshold_now(Q.bsf2, m);
+  const float b2 =
+      enumerate_all ? __int_as_float(0x7f800000) : prune_threshold_now(Q.bsf2 + T.series, m);
   const double twoB = 2.0 * sqrt((double)b2);
 
   // ---- exact anchors at the tile's first row ----
@@ -101,7 +104,6 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_lb(DevSeries S, DevSearch Q,
     }
   }
 
-  unsigned int npairs = 0, nfast = 0;
   double w1[kLbPerThread], w2[kLbPerThread], w3[kLbPerThread], w4[kLbPerThread];
   double ws[kLbPerThread], wg[kLbPerThread];
   for (int st = 0; st < T.rows; st += kStage) {
@@ -162,8 +164,8 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_lb(DevSeries S, DevSearch Q,
             Cr[l] = fma(w3[sl], q2, Cr[l]);
           }
           const bool valid = row_ok && i + Lt + l < s;
-          const bool prune = !enumerate_all &&
-                             (fma(qg, ws[sl], -Cf[l]) > 0.0 || fma(wg[sl], qs, -Cr[l]) > 0.0);
+          // with the bounds off (best-so-far +inf) only flat windows prune
+          const bool prune = fma(qg, ws[sl], -Cf[l]) > 0.0 || fma(wg[sl], qs, -Cr[l]) > 0.0;
           npairs += valid ? 1u : 0u;
           nfast += (valid && prune) ? 1u : 0u;
           word[l] |= (valid && !prune ? 1u : 0u) << (r & 31);
@@ -192,6 +194,28 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_lb(DevSeries S, DevSearch Q,
 #pragma unroll
     for (int l = 0; l < kLbPerThread; ++l) out[(size_t)(t * kLbPerThread + l) * kLbWords + wi] = 0u;
   }
+}
+
+// Persistent sweep: each CTA takes tiles from the work counter *next until
+// the chunk is exhausted; tile k of the chunk writes its bits to slot k.
+__global__ void __launch_bounds__(kLbThreads, 2) k_lb(DevSeries S, DevSearch Q,
+                                                      const Tile* tiles, int ntiles,
+                                                      unsigned int* bits, bool enumerate_all,
+                                                      unsigned int* next) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  LbShared& sh = *reinterpret_cast<LbShared*>(smraw);
+  __shared__ unsigned int tile_idx;
+  const int lane = threadIdx.x & 31;
+  unsigned int npairs = 0, nfast = 0;
+  for (;;) {
+    __syncthreads();  // every thread has read tile_idx and left the previous tile's staging
+    if (threadIdx.x == 0) tile_idx = atomicAdd(next, 1u);
+    __syncthreads();
+    const unsigned int k = tile_idx;
+    if (k >= (unsigned int)ntiles) break;
+    const Tile T = tiles[k];
+    lb_tile(S, Q, T, bits + (size_t)k * kLbLags * kLbWords, enumerate_all, sh, npairs, nfast);
+  }
   unsigned long long np = npairs, nf = nfast;
   for (int o = 16; o > 0; o >>= 1) {
     np += __shfl_xor_sync(0xffffffffu, np, o);
@@ -208,15 +232,18 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_lb(DevSeries S, DevSearch Q,
 size_t lb_smem_bytes() { return sizeof(LbShared); }
 
 void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
-               int tile_end, unsigned int* bits, bool enumerate_all, cudaStream_t st) {
+               int tile_end, unsigned int* bits, bool enumerate_all, unsigned int* next,
+               int num_sms, cudaStream_t st) {
   if (tile_end <= tile_begin) return;
   static bool configured = false;
   if (!configured) {
     cudaFuncSetAttribute(k_lb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LbShared));
     configured = true;
   }
-  k_lb<<<tile_end - tile_begin, kLbThreads, sizeof(LbShared), st>>>(S, Q, tiles + tile_begin,
-                                                                     bits, enumerate_all);
+  const int ntiles = tile_end - tile_begin;
+  const int resident = 2 * num_sms;  // two CTAs per SM (launch bounds, shared memory)
+  k_lb<<<ntiles < resident ? ntiles : resident, kLbThreads, sizeof(LbShared), st>>>(
+      S, Q, tiles + tile_begin, ntiles, bits, enumerate_all, next);
 }
 
 }  // namespace dtwj

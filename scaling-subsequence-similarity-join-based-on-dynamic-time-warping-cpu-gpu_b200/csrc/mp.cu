@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
   extern __shared__ __align__(16) unsigned char smraw[];
   MpShared& sh = *reinterpret_cast<MpShared*>(smraw);
   const Tile T = tiles[blockIdx.x];
-  const int64_t s = S.s;
+  const int64_t s = T.send;  // windows of the tile's series end here
   const int m = S.m;
   const int t = threadIdx.x, lane = t & 31;
   const int64_t L0 = T.L0, i0 = T.i0;
@@ -204,11 +204,17 @@ __global__ void __launch_bounds__(kSelThreads) k_seed_select(DevSeries S,
                                                               const unsigned long long* keys,
                                                               int2* seeds, unsigned int* nseeds,
                                                               unsigned int* bsf2) {
+  // block b selects the seeds of series b (windows [wb, we))
+  const int b = blockIdx.x;
+  const int64_t wb = S.sbeg ? S.sbeg[b] : 0;
+  const int64_t we = S.sbeg ? S.sbeg[b + 1] - S.m + 1 : S.s;
+  seeds += (size_t)b * kSeeds;
+  for (int x = threadIdx.x; x < kSeeds; x += blockDim.x) seeds[x] = make_int2(-1, -1);
   unsigned long long loc[kLocal];
   int part[kLocal];
 #pragma unroll
   for (int q = 0; q < kLocal; ++q) { loc[q] = ULLONG_MAX; part[q] = -1; }
-  for (int64_t i = threadIdx.x; i < S.s; i += blockDim.x) {
+  for (int64_t i = wb + threadIdx.x; i < we; i += blockDim.x) {
     const unsigned long long k = keys[i];
     if (k == ULLONG_MAX) continue;
     const unsigned long long sk = (k & 0xffffffff00000000ull) | (unsigned long long)(unsigned int)i;
@@ -270,14 +276,14 @@ __global__ void __launch_bounds__(kSelThreads) k_seed_select(DevSeries S,
       if (round == 0) {
         const unsigned long long bits = ((wn >> 32) + 1ull) << 32;
         const float e2 = __double2float_ru(__longlong_as_double((long long)bits));
-        *bsf2 = __float_as_uint(e2);
+        bsf2[b] = __float_as_uint(e2);
       }
       ++head;
     }
     ++count;
     __syncthreads();
   }
-  if (threadIdx.x == 0) *nseeds = count;
+  if (threadIdx.x == 0) nseeds[b] = count;
 }
 
 __global__ void k_reverse(const double* a, int64_t n, double* out) {
@@ -316,7 +322,7 @@ void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
 
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
                         unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st) {
-  k_seed_select<<<1, kSelThreads, 0, st>>>(S, keys, seeds, nseeds, bsf2);
+  k_seed_select<<<S.nseries, kSelThreads, 0, st>>>(S, keys, seeds, nseeds, bsf2);
 }
 
 }  // namespace dtwj

@@ -248,9 +248,12 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
     idx = __shfl_sync(gm, idx, 0, G);
     if (idx >= total) break;
     const int2 pr = pairs[idx];
+    if (pr.x < 0) continue;  // an unused seed slot
     const int64_t i = pr.x, j = pr.y;
+    const int sr = series_of(S, i);
+    unsigned int* bsf2 = Q.bsf2 + sr;
     const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
-    float thr = prune_threshold_now(Q.bsf2, S.m);
+    float thr = prune_threshold_now(bsf2, S.m);
     for (int x = g; x <= lay.nc + 1; x += G) cbc[x] = 0.0f;
     if (!bounds) {
       for (int k = g; k < m; k += G) {
@@ -388,23 +391,23 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
     unsigned long long cells = 0;
     bool ab = false;
     const float d2 =
-        dtw_band<float, C, G, true>(q, t, m, w, cbc, lay.nc, thr, Q.bsf2, gm, g, &cells, &ab);
+        dtw_band<float, C, G, true>(q, t, m, w, cbc, lay.nc, thr, bsf2, gm, g, &cells, &ab);
     if (g == 0) {
       atomicAdd(&cnt[kDtwCalls], 1ull);
       atomicAdd(&cnt[kDtwCells], cells);
       if (ab) {
         atomicAdd(&cnt[kDtwAbandoned], 1ull);
       } else {
-        const float now = prune_threshold_now(Q.bsf2, S.m);
+        const float now = prune_threshold_now(bsf2, S.m);
         if (d2 <= now) {
-          atomicMin(Q.bsf2, __float_as_uint(d2));
+          atomicMin(bsf2, __float_as_uint(d2));
           const unsigned int slot = atomicAdd(Q.cand_count, 1u);
           if (slot < Q.cand_cap) {
             Candidate cd;
             cd.i = (int)i;
             cd.j = (int)j;
             cd.d2 = d2;
-            cd.pad = 0;
+            cd.series = sr;
             Q.cand[slot] = cd;
           }
         }
@@ -449,14 +452,13 @@ __global__ void __launch_bounds__(128) k_dtw_list(DevSeries S, const int2* pairs
     const unsigned int c = *count_ptr;
     n = (int)(c < (unsigned)count ? c : (unsigned)count);
   }
-  const float fin = bsf2 ? prune_threshold(*bsf2, S.m) : 0.0f;
   for (int k = blockIdx.x * groups + gib; k < n; k += gridDim.x * groups) {
     int64_t i, j;
     if (cands) {
       const Candidate cd = cands[k];
       i = cd.i;
       j = cd.j;
-      if (bsf2 && cd.d2 > fin) {
+      if (bsf2 && cd.d2 > prune_threshold(bsf2[cd.series], S.m)) {
         if (g == 0) out[k] = __longlong_as_double(0x7ff0000000000000LL);
         continue;
       }
@@ -479,62 +481,45 @@ __global__ void __launch_bounds__(128) k_dtw_list(DevSeries S, const int2* pairs
   }
 }
 
-// Lexicographic minimum (d2, i, j) over the verified candidates.
-__global__ void k_best(const Candidate* cands, const unsigned int* count_ptr, int cap,
-                       const double* d2, double* out_d2, int* out_idx) {
+// Per series lexicographic minimum (d2, i, j) over the verified candidates,
+// in three passes of atomicMin on 64-bit keys (non-negative doubles order
+// like their bit patterns): the distance, then i << 32 | j among the
+// candidates at that distance, then the FP32 search distance of that pair.
+__global__ void k_best_d2(const Candidate* cands, const unsigned int* count_ptr, int cap,
+                          const double* d2, unsigned long long* best_d2) {
   const unsigned int c = *count_ptr;
   const int n = (int)(c < (unsigned)cap ? c : (unsigned)cap);
-  __shared__ double bd[32];
-  __shared__ int bk[32];
-  const double INF = __longlong_as_double(0x7ff0000000000000LL);
-  double best = INF;
-  int bi = -1;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const double v = d2[k];
-    if (!(v < INF)) continue;
-    if (bi < 0 || v < best ||
-        (v == best && (cands[k].i < cands[bi].i ||
-                       (cands[k].i == cands[bi].i && cands[k].j < cands[bi].j)))) {
-      best = v;
-      bi = k;
-    }
+    if (v < __longlong_as_double(0x7ff0000000000000LL))
+      atomicMin(best_d2 + cands[k].series, (unsigned long long)__double_as_longlong(v));
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-    const int ok = __shfl_xor_sync(0xffffffffu, bi, o);
-    bool take = false;
-    if (ok >= 0) {
-      if (bi < 0 || ov < best) take = true;
-      else if (ov == best && (cands[ok].i < cands[bi].i ||
-                              (cands[ok].i == cands[bi].i && cands[ok].j < cands[bi].j)))
-        take = true;
-    }
-    if (take) {
-      best = ov;
-      bi = ok;
-    }
+}
+
+__global__ void k_best_ij(const Candidate* cands, const unsigned int* count_ptr, int cap,
+                          const double* d2, const unsigned long long* best_d2,
+                          unsigned long long* best_ij) {
+  const unsigned int c = *count_ptr;
+  const int n = (int)(c < (unsigned)cap ? c : (unsigned)cap);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const Candidate cd = cands[k];
+    if ((unsigned long long)__double_as_longlong(d2[k]) == best_d2[cd.series])
+      atomicMin(best_ij + cd.series,
+                ((unsigned long long)(unsigned int)cd.i << 32) | (unsigned int)cd.j);
   }
-  if ((threadIdx.x & 31) == 0) {
-    bd[threadIdx.x >> 5] = best;
-    bk[threadIdx.x >> 5] = bi;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double b = __longlong_as_double(0x7ff0000000000000LL);
-    int k = -1;
-    for (int x = 0; x < (int)(blockDim.x >> 5); ++x) {
-      const int ok = bk[x];
-      if (ok < 0) continue;
-      const double ov = bd[x];
-      if (k < 0 || ov < b ||
-          (ov == b && (cands[ok].i < cands[k].i ||
-                       (cands[ok].i == cands[k].i && cands[ok].j < cands[k].j)))) {
-        b = ov;
-        k = ok;
-      }
-    }
-    *out_d2 = b;
-    *out_idx = k;
+}
+
+__global__ void k_best_f32(const Candidate* cands, const unsigned int* count_ptr, int cap,
+                           const double* d2, const unsigned long long* best_d2,
+                           const unsigned long long* best_ij, unsigned int* best_f32) {
+  const unsigned int c = *count_ptr;
+  const int n = (int)(c < (unsigned)cap ? c : (unsigned)cap);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const Candidate cd = cands[k];
+    const unsigned long long ij = ((unsigned long long)(unsigned int)cd.i << 32) | (unsigned int)cd.j;
+    if ((unsigned long long)__double_as_longlong(d2[k]) == best_d2[cd.series] &&
+        ij == best_ij[cd.series])
+      atomicMin(best_f32 + cd.series, __float_as_uint(cd.d2));
   }
 }
 
@@ -643,7 +628,8 @@ void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
 }
 
 void launch_verify(const DevSeries& S, const DevSearch& Q, BandShape band, double* out_d2,
-                   double* best_d2, int* best_idx, cudaStream_t st) {
+                   unsigned long long* best_d2, unsigned long long* best_ij, float* best_f32,
+                   cudaStream_t st) {
 #define X(c, g)                                                                          \
   if (band.C == c && band.G == g) {                                                      \
     run_list<double, c, g>(S, nullptr, Q.cand, Q.cand_count, (int)Q.cand_cap, Q.bsf2,   \
@@ -651,7 +637,15 @@ void launch_verify(const DevSeries& S, const DevSearch& Q, BandShape band, doubl
   }
   DTWJ_BAND_CASES(X)
 #undef X
-  k_best<<<1, 256, 0, st>>>(Q.cand, Q.cand_count, (int)Q.cand_cap, out_d2, best_d2, best_idx);
+  const int ns = S.nseries;
+  cudaMemsetAsync(best_d2, 0xff, (size_t)ns * 8, st);
+  cudaMemsetAsync(best_ij, 0xff, (size_t)ns * 8, st);
+  cudaMemsetAsync(best_f32, 0xff, (size_t)ns * 4, st);
+  const int cap = (int)Q.cand_cap;
+  k_best_d2<<<256, 256, 0, st>>>(Q.cand, Q.cand_count, cap, out_d2, best_d2);
+  k_best_ij<<<256, 256, 0, st>>>(Q.cand, Q.cand_count, cap, out_d2, best_d2, best_ij);
+  k_best_f32<<<256, 256, 0, st>>>(Q.cand, Q.cand_count, cap, out_d2, best_d2, best_ij,
+                                  reinterpret_cast<unsigned int*>(best_f32));
 }
 
 void launch_pair_dtw(const DevSeries& S, const int2* pairs, int count, bool precise,

@@ -35,6 +35,20 @@ __global__ void k_check_finite(const double* a, int64_t n, int* status) {
   }
 }
 
+// Series of every sample of a batch: the r with sbeg[r] <= p < sbeg[r + 1].
+__global__ void k_series_ids(const int64_t* sbeg, int nseries, int* sid, int64_t n) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nseries - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sbeg[mid] <= p) lo = mid;
+      else hi = mid - 1;
+    }
+    sid[p] = lo;
+  }
+}
+
 // Exact two-pass mean and population deviation of each window, FP64.
 __global__ void k_stats(DevSeries S) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -57,12 +71,19 @@ __global__ void k_stats(DevSeries S) {
   S.flat[i] = flat ? 1 : 0;
 }
 
-// Clipped Sakoe-Chiba envelope of the raw series: U[p] = max a[p-w .. p+w].
+// Clipped Sakoe-Chiba envelope of the raw series: U[p] = max a[p-w .. p+w],
+// clipped to the sample's own series in a batch.
 __global__ void k_envelope(DevSeries S) {
   const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= S.n) return;
-  const int64_t lo = p - S.w > 0 ? p - S.w : 0;
-  const int64_t hi = p + S.w < S.n - 1 ? p + S.w : S.n - 1;
+  int64_t b = 0, e = S.n;
+  if (S.sid) {
+    const int r = S.sid[p];
+    b = S.sbeg[r];
+    e = S.sbeg[r + 1];
+  }
+  const int64_t lo = p - S.w > b ? p - S.w : b;
+  const int64_t hi = p + S.w < e - 1 ? p + S.w : e - 1;
   double u = S.a[lo], l = S.a[lo];
   for (int64_t q = lo + 1; q <= hi; ++q) {
     double v = S.a[q];
@@ -302,6 +323,10 @@ __global__ void k_mask(DevSeries S, const double* diff, const double* mean_acc) 
 }
 
 }  // namespace
+
+void launch_series_ids(const int64_t* sbeg, int nseries, int* sid, int64_t n, cudaStream_t st) {
+  k_series_ids<<<1024, 256, 0, st>>>(sbeg, nseries, sid, n);
+}
 
 void launch_check_finite(const double* a, int64_t n, int* status, cudaStream_t st) {
   unsigned g = grid_for(n);

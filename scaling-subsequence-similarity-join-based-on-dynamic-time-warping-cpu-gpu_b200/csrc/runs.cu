@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
     const Tile T = tiles[item / kLbLags];
     const int64_t L = (int64_t)T.L0 + (int64_t)(item % kLbLags);
     // rows this lag really has in the tile: r < rows and i0 + r + L < s
-    int64_t nrow = S.s - L - T.i0;
+    int64_t nrow = (int64_t)T.send - L - T.i0;
     if (nrow > T.rows) nrow = T.rows;
     bool nz = false;
     for (int x = lane; x < kLbWords; x += 32) {
@@ -261,7 +261,8 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
       }
       continue;
     }
-    float thr = prune_threshold_now(Q.bsf2, S.m);
+    const unsigned int* bsf2 = Q.bsf2 + T.series;
+    float thr = prune_threshold_now(bsf2, S.m);
     // ---- masked sums at the run's first pair (exact, FP64) ----
     double F1 = 0, F2 = 0, F3 = 0, R1 = 0, R2 = 0, R3 = 0;
     if (masked) {
@@ -338,14 +339,14 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
         if (alive) {
           const unsigned int slot = base + __popc(bits & ((1u << lane) - 1u));
           if (slot < Q.kq_cap) {
-            Q.kq[slot] = make_int4((int)i, (int)j, __float_as_int(kim), 0);
+            Q.kq[slot] = make_int4((int)i, (int)j, __float_as_int(kim), T.series);
           } else {
             atomicOr(S.status, 2);
           }
         }
       }
       // a fresh best-so-far tightens the rest of the run
-      thr = fminf(thr, prune_threshold_now(Q.bsf2, S.m));
+      thr = fminf(thr, prune_threshold_now(bsf2, S.m));
     }
       }
       __syncwarp();
@@ -367,6 +368,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
 __global__ void __launch_bounds__(kKeoghWarps * 32, 5) k_keogh(DevSeries S, DevSearch Q) {
   __shared__ KeoghSide side[kKeoghWarps][kKeoghBatch][2];
   __shared__ float endsv[kKeoghWarps][kKeoghBatch][2];
+  __shared__ int serv[kKeoghWarps][kKeoghBatch];
   __shared__ unsigned long long pruned_block;
   if (threadIdx.x == 0) pruned_block = 0;
   __syncthreads();
@@ -406,10 +408,11 @@ __global__ void __launch_bounds__(kKeoghWarps * 32, 5) k_keogh(DevSeries S, DevS
         t = fma(dd, dd, t);
       }
       endsv[warp][e][d] = (float)fmax((double)__int_as_float(r.z), t);
+      if (d == 0) serv[warp][e] = r.w;
     }
     __syncwarp();
-    const float thr = prune_threshold_now(Q.bsf2, S.m);
     for (int e = 0; e < cnt; ++e) {
+      const float thr = prune_threshold_now(Q.bsf2 + serv[warp][e], S.m);
       const KeoghSide& wi = side[warp][e][0];
       const KeoghSide& wj = side[warp][e][1];
       bool live = keogh_within(S, wi, wj, endsv[warp][e][0], thr, lane);

@@ -95,8 +95,17 @@ def test_flat_windows_are_excluded(gpu_dtwj, oracle, synth):
     x = synth.random_walk(3000, 7)
     x[1000:1200] = 5.0
     ref = oracle.join(x, 64, 4)
-    r = gpu_dtwj.join(x, 64, 4)
-    _check(r, ref.i, ref.j, ref.dist)
+    # with the bounds off as well: flat windows never reach the DTW stage
+    for flags in (0, gpu_dtwj.F_NO_DIAG):
+        r = gpu_dtwj.join(x, 64, 4, flags)
+        _check(r, ref.i, ref.j, ref.dist)
+
+
+def test_all_flat_series_has_no_pair(gpu_dtwj):
+    # no valid window at all: the best-so-far stays +inf and nothing may reach
+    # the DTW stage
+    r = gpu_dtwj.join(np.full(4000, -1.25), 64, 4)
+    assert (r.i, r.j) == (-1, -1) and not np.isfinite(r.dist)
 
 
 def test_exact_duplicate_resolves_to_lowest_index(gpu_dtwj, synth):
