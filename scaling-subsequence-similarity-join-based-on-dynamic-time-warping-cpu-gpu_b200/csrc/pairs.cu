@@ -41,6 +41,13 @@ template <> struct Pad<double> {
 };
 
 __device__ __forceinline__ float fmin_(float a, float b) { return fminf(a, b); }
+// min(a, b, c) in one instruction for FP32 (three-input min.f32, sm_100).
+__device__ __forceinline__ float fmin3_(float a, float b, float c) {
+  float d;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ double fmin3_(double a, double b, double c) { return fmin(fmin(a, b), c); }
 __device__ __forceinline__ double fmin_(double a, double b) { return fmin(a, b); }
 __device__ __forceinline__ float fmax_(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double fmax_(double a, double b) { return fmax(a, b); }
@@ -63,8 +70,7 @@ __device__ __forceinline__ V group_sum(V v, unsigned int gm) {
 struct GroupLayout {
   int pq, pt;     // padding of q and t on each side
   int nc;         // cumulative-bound chunks
-  int e2;         // edge prefix/suffix length
-  int q_off, t_off, cb_off, edge_off, total;
+  int q_off, t_off, cb_off, total;
 };
 
 __host__ __device__ inline GroupLayout group_layout(int m, int w, int C, int G, bool bounds) {
@@ -72,13 +78,10 @@ __host__ __device__ inline GroupLayout group_layout(int m, int w, int C, int G, 
   l.pq = G + 1;
   l.pt = G * C + G + 2;  // t is read at offsets [-(G + w), m + G + GC)
   l.nc = (m + 7) / 8;
-  l.e2 = m < 2 * w ? m : 2 * w;
-  if (l.e2 < 1) l.e2 = 1;
   l.q_off = l.pq;
   l.t_off = l.pq + m + l.pq + l.pt;
   l.cb_off = l.t_off + m + l.pt;
-  l.edge_off = l.cb_off + l.nc + 2;
-  l.total = l.edge_off + (bounds ? 8 * l.e2 : 0);
+  l.total = l.cb_off + l.nc + 2;
   l.total = (l.total + 3) & ~3;
   return l;
 }
@@ -113,7 +116,7 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
     const T qr = q[r];
     {
       const T d = qr - tw[0];
-      T v = fmin_(fmin_(prev[1 < C ? 1 : 0], prev[0]), left);
+      T v = fmin3_(prev[1 < C ? 1 : 0], prev[0], left);
       v = fmax_(fma(d, d, v), pen[0]);
       cur[0] = v;
     }
@@ -123,7 +126,7 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
     for (int c = 1; c < C; ++c) {
       const T up = (c + 1 < C) ? prev[c + 1 < C ? c + 1 : 0] : right;
       const T d = qr - tw[c];
-      T v = fmin_(fmin_(up, prev[c]), cur[c - 1]);
+      T v = fmin3_(up, prev[c], cur[c - 1]);
       v = fmax_(fma(d, d, v), pen[c]);
       cur[c] = v;
     }
@@ -180,37 +183,6 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
   return result;
 }
 
-// Envelope of z-normalised window `sub` (subs_U / subs_L of the reference) at
-// offset k: raw envelope in the interior, prefix / suffix extremes of the
-// window near its ends (the clipped window of lower_upper_lemire).
-struct EdgeEnv {
-  const float *pu, *pl, *su, *sl;  // prefix max/min [0, e2), suffix max/min [m-e2, m)
-  int e2;
-};
-
-__device__ __forceinline__ void envelope_at(const DevSeries& S, int64_t sub, double mu,
-                                            double isg, const EdgeEnv& E, int k, float* U,
-                                            float* L) {
-  const int m = S.m, w = S.w;
-  if (k < w) {
-    const int p = k + w < m - 1 ? k + w : m - 1;
-    *U = E.pu[p];
-    *L = E.pl[p];
-  } else if (k > m - 1 - w) {
-    const int p = (k - w > 0 ? k - w : 0) - (m - E.e2);
-    *U = E.su[p];
-    *L = E.sl[p];
-  } else {
-    *U = (float)((S.U[sub + k] - mu) * isg);
-    *L = (float)((S.L[sub + k] - mu) * isg);
-  }
-}
-
-__device__ __forceinline__ float keogh_term(float x, float U, float L) {
-  const float du = x - U, dl = x - L;
-  return x > U ? du * du : (x < L ? dl * dl : 0.0f);
-}
-
 // The pair consumer: every group takes pairs from the queue until it is
 // drained.  flags bit 0: run the bounds (otherwise DTW only, for seeds).
 template <int C, int G>
@@ -229,7 +201,6 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
   float* q = base + lay.q_off;
   float* t = base + lay.t_off;
   float* cbc = base + lay.cb_off;
-  float* edge = base + lay.edge_off;
   for (int x = threadIdx.x; x < kNumCounters; x += blockDim.x) cnt[x] = 0;
   // sentinels (written once; the interior is rewritten per pair)
   for (int x = g; x < lay.pq; x += G) {
@@ -262,14 +233,8 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
       }
       __syncwarp(gm);
     } else {
-      // ---- window ends first: endpoint bound and clipped edge envelopes ----
-      const int e2 = lay.e2;
-      const int tail = m - e2 > e2 ? m - e2 : e2;  // first position of the tail region
-      for (int k = g; k < e2; k += G) {
-        q[k] = (float)((S.a[i + k] - mi) * si);
-        t[k] = (float)((S.a[j + k] - mj) * sj);
-      }
-      for (int k = tail + g; k < m; k += G) {
+      // ---- z-normalised windows and the endpoint bound's two parts ----
+      for (int k = g; k < m; k += G) {
         q[k] = (float)((S.a[i + k] - mi) * si);
         t[k] = (float)((S.a[j + k] - mj) * sj);
       }
@@ -278,114 +243,52 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
       if (g == 0) kim_bound<float>(q, t, m, &kl, &kr);
       kl = __shfl_sync(gm, kl, 0, G);
       kr = __shfl_sync(gm, kr, 0, G);
-      if (kl + kr > thr) {
-        if (g == 0) atomicAdd(&cnt[kPrunedKim], 1ull);
-        __syncwarp(gm);
-        continue;
-      }
-      for (int sc = g; sc < 8; sc += G) {
-        const float* z = (sc >> 2) ? t : q;
-        float* out = edge + sc * e2;
-        const int kind = sc & 3;
-        if (kind < 2) {
-          float acc = z[0];
-          for (int p = 0; p < e2; ++p) {
-            acc = kind == 0 ? fmaxf(acc, z[p]) : fminf(acc, z[p]);
-            out[p] = acc;
-          }
-        } else {
-          float acc = z[m - 1];
-          for (int p = m - 1; p >= m - e2; --p) {
-            acc = kind == 2 ? fmaxf(acc, z[p]) : fminf(acc, z[p]);
-            out[p - (m - e2)] = acc;
-          }
-        }
-      }
-      __syncwarp(gm);
-      // edge layout: [0..3] window i: pu, pl, su, sl; [4..7] window j
-      const EdgeEnv Ei = {edge, edge + e2, edge + 2 * e2, edge + 3 * e2, e2};
-      const EdgeEnv Ej = {edge + 4 * e2, edge + 5 * e2, edge + 6 * e2, edge + 7 * e2, e2};
-      // ---- LB_Keogh both directions (LB_KK, lb_keogh.cpp:9-72), in rounds of
-      // 8G positions with early abandoning; the middle of both windows is
-      // z-normalised into shared memory on the way ----
-      float e1 = 0, m1 = 0, e2s = 0, m2 = 0;
-      bool dead = false;
-      for (int base = 0; base < m && !dead; base += 8 * G) {
-        const int lim = base + 8 * G < m ? base + 8 * G : m;
-        for (int k = base + g; k < lim; k += G) {
-          float qk, tk;
-          if (k >= e2 && k < tail) {
-            qk = (float)((S.a[i + k] - mi) * si);
-            tk = (float)((S.a[j + k] - mj) * sj);
-            q[k] = qk;
-            t[k] = tk;
-          } else {
-            qk = q[k];
-            tk = t[k];
-          }
-          float U, Lw;
-          envelope_at(S, j, mj, sj, Ej, k, &U, &Lw);
-          const float a1 = keogh_term(qk, U, Lw);
-          envelope_at(S, i, mi, si, Ei, k, &U, &Lw);
-          const float a2 = keogh_term(tk, U, Lw);
+      // ---- cumulative bound for abandoning: LB_Keogh terms of the rows (q)
+      // against the envelope of window j, in 8-row chunks, suffix-summed.
+      // Lane g owns chunks [g per, g per + per): it sums its block from the
+      // end, then adds the totals of the lanes above it (suffix scan). ----
+      const int per = (lay.nc + G - 1) / G;
+      float run = 0.0f;
+      for (int u = per - 1; u >= 0; --u) {
+        const int x = g * per + u;
+        if (x >= lay.nc) continue;
+        float acc = 0.0f;
+        const int k1 = 8 * x + 8 < m ? 8 * x + 8 : m;
+        for (int k = 8 * x; k < k1; ++k) {
           if (k < kBias || k >= m - kBias) {
-            e1 += a1;
-            e2s += a2;
+            acc += k == 0 ? kl : (k == m - kBias ? kr : 0.0f);
           } else {
-            m1 += a1;
-            m2 += a2;
+            const float U = (float)((S.U[j + k] - mj) * sj), L = (float)((S.L[j + k] - mj) * sj);
+            const float d = fmaxf(fmaxf(q[k] - U, L - q[k]), 0.0f);
+            acc = fmaf(d, d, acc);
           }
         }
-        const float p1 = fmaxf(group_sum<G>(e1, gm), kl + kr) + group_sum<G>(m1, gm);
-        const float p2 = fmaxf(group_sum<G>(e2s, gm), kl + kr) + group_sum<G>(m2, gm);
-        if (p1 > thr || p2 > thr) dead = true;
+        run += acc;
+        cbc[x] = run;
       }
-      if (dead) {
-        if (g == 0) atomicAdd(&cnt[kPrunedKeogh], 1ull);
-        __syncwarp(gm);
-        continue;
+      float above = run;  // inclusive suffix scan of the lane totals
+#pragma unroll
+      for (int o = 1; o < G; o <<= 1) {
+        const float v = __shfl_down_sync(gm, above, o, G);
+        if (g + o < G) above += v;
       }
-      e1 = group_sum<G>(e1, gm);
-      m1 = group_sum<G>(m1, gm);
-      e2s = group_sum<G>(e2s, gm);
-      m2 = group_sum<G>(m2, gm);
-      const float lb1 = fmaxf(e1, kl + kr) + m1;
-      const float lb2 = fmaxf(e2s, kl + kr) + m2;
-      __syncwarp(gm);
-      // ---- cumulative bound of the larger direction, 8-cell chunks ----
-      const bool dir1 = lb1 > lb2;
-      for (int x = g; x < lay.nc; x += G) {
-        float acc = 0.0f;
-        for (int k = 8 * x; k < 8 * x + 8 && k < m; ++k) {
-          float v;
-          if (k == 0) v = kl;
-          else if (k == m - kBias) v = kr;
-          else if (k < kBias || k >= m - kBias) v = 0.0f;
-          else {
-            float U, Lw;
-            if (dir1) {
-              envelope_at(S, j, mj, sj, Ej, k, &U, &Lw);
-              v = keogh_term(q[k], U, Lw);
-            } else {
-              envelope_at(S, i, mi, si, Ei, k, &U, &Lw);
-              v = keogh_term(t[k], U, Lw);
-            }
-          }
-          acc += v;
-        }
-        cbc[x] = acc;
+      above -= run;
+      for (int u = 0; u < per; ++u) {
+        const int x = g * per + u;
+        if (x < lay.nc) cbc[x] += above;
       }
-      __syncwarp(gm);
       if (g == 0) {
-        float acc = 0.0f;
-        for (int x = lay.nc - 1; x >= 0; --x) {
-          acc += cbc[x];
-          cbc[x] = acc;
-        }
         cbc[lay.nc] = 0.0f;
         cbc[lay.nc + 1] = 0.0f;
       }
       __syncwarp(gm);
+      // the whole bound (LB_Keogh of q against j's envelope with the endpoint
+      // parts) already exceeds the best-so-far: no DTW
+      if (cbc[0] > thr) {
+        if (g == 0) atomicAdd(&cnt[kPrunedKeogh], 1ull);
+        __syncwarp(gm);
+        continue;
+      }
     }
     // ---- banded DTW (FP32, early abandoning) ----
     unsigned long long cells = 0;
