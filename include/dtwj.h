@@ -61,6 +61,9 @@ extern "C" {
 #define DTWJ_F_LEARNED 0x8u     /* order the tile queue with the loaded MLP   */
 #define DTWJ_F_VERBOSE 0x10u    /* phase timings on stderr                    */
 #define DTWJ_F_PROFILE 0x20u    /* per-phase device times (CUDA events)       */
+#define DTWJ_F_NO_GRAPH 0x40u   /* launch the sweep directly, not as a CUDA graph
+                                   (by default a context captures the sweep once and
+                                   replays it while its launches are unchanged) */
 
 /* phases reported in dtwj_result.phase_seconds / phase_launches */
 #define DTWJ_PHASE_PREP 0       /* statistics, envelopes, mask, row terms     */

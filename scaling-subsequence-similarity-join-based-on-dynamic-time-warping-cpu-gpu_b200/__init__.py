@@ -42,6 +42,7 @@ F_NO_DIAG = 0x4
 F_LEARNED = 0x8
 F_VERBOSE = 0x10
 F_PROFILE = 0x20
+F_NO_GRAPH = 0x40
 
 PHASES = ("prep", "profile", "seeds", "diag", "pairs", "verify", "runs", "keogh")
 

@@ -59,6 +59,12 @@ struct dtwj_ctx {
   int64_t lbtiles_n = -1, lbtiles_m = -1;  // single-series shape the tiles were built for
   std::vector<unsigned int> host_u32;      // staging of small host -> device copies
   std::vector<cudaEvent_t> pool;  // events for per-phase device times
+  // the sweep's launches captured as a CUDA graph, replayed while every
+  // launch argument is unchanged (same buffers, tiles, band, flags)
+  cudaGraphExec_t sweep_exec = nullptr;
+  std::vector<unsigned char> sweep_key;
+  std::vector<int> sweep_marks;  // phase marks of the capture: (phase, a, b, launches)
+  size_t sweep_ev0 = 0, sweep_ev1 = 0;
 };
 
 namespace {
@@ -131,21 +137,32 @@ struct Phases {
     }
     return ctx->pool[k];
   }
+  // While the stream is being captured, records are external: they become
+  // event-record nodes of the graph (a plain record would only order the
+  // capture, and the external flag is refused outside a capture).
+  bool capturing = false;
+  void record(cudaEvent_t e) {
+    if (capturing) cudaEventRecordWithFlags(e, ctx->stream, cudaEventRecordExternal);
+    else cudaEventRecord(e, ctx->stream);
+  }
   void begin() {
     if (!on) return;
     open_at = used;
-    cudaEventRecord(ev(used++), ctx->stream);
+    record(ev(used++));
   }
   void end(int phase, int launches) {
     if (!on) return;
-    cudaEventRecord(ev(used), ctx->stream);
+    record(ev(used));
     marks.push_back({phase, open_at, used, launches});
     ++used;
   }
   void collect(dtwj_result* out) {
     for (auto& mk : marks) {
       float ms = 0.f;
-      cudaEventElapsedTime(&ms, ctx->pool[mk.a], ctx->pool[mk.b]);
+      if (cudaEventElapsedTime(&ms, ctx->pool[mk.a], ctx->pool[mk.b]) != cudaSuccess) {
+        cudaGetLastError();  // a mark without a time must not fail the next call
+        ms = 0.f;
+      }
       out->phase_seconds[mk.phase] += ms / 1000.0;
       out->phase_launches[mk.phase] += (uint64_t)mk.launches;
     }
@@ -254,7 +271,29 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
     ENSURE(B_DIFF, n * 8, diff);
     ENSURE(B_MEAN, 8, mean);
     ENSURE(B_ZMAX, 4, zmax);
-    launch_mask(S, counts, lt_max, diff, mean, zmax, st);
+    if (!sbeg_host) {
+      launch_mask(S, counts, lt_max, diff, mean, zmax, st);
+    } else {
+      // the mask's CDF tables are per series: build it on a view of each one
+      for (int r = 0; r < nseries; ++r) {
+        const int64_t b = sbeg_host[r], nr = sbeg_host[r + 1] - b;
+        DevSeries V = S;
+        V.a = S.a + b;
+        V.n = nr;
+        V.s = nr - m + 1;
+        V.mu = S.mu + b;
+        V.sig = S.sig + b;
+        V.isg = S.isg + b;
+        V.flat = S.flat + b;
+        V.U = S.U + b;
+        V.L = S.L + b;
+        V.mask = S.mask + b;
+        V.sid = nullptr;
+        V.sbeg = nullptr;
+        V.nseries = 1;
+        launch_mask(V, counts, lt_max, diff, mean, zmax, st);
+      }
+    }
   } else {
     CUDA_OK(cudaMemsetAsync(S.mask, 0, n * 4, st));
   }
@@ -279,8 +318,7 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   BandShape band;
   if (!choose_band(w, &band)) return DTWJ_ERR_BAND;
   if (flags & DTWJ_F_LEARNED) return DTWJ_ERR_NOMODEL;
-  // the masked bound's CDF tables are per series; batches go without it
-  const bool masked = !sbeg && !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
+  const bool masked = !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
   const bool verbose = flags & DTWJ_F_VERBOSE;
   cudaStream_t st = ctx->stream;
   Phases ph(ctx, (flags & DTWJ_F_PROFILE) != 0);
@@ -367,9 +405,10 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   if (enumerate_all) chunk = (int)((double)qcap / tile_pairs) > 0 ? (int)((double)qcap / tile_pairs) : 1;
   unsigned int* bits;
   ENSURE(B_BITS, (size_t)(chunk < nlb ? chunk : (nlb > 0 ? nlb : 1)) * kLbLags * kLbWords * 4, bits);
-  for (int attempt = 0;; ++attempt) {
-    for (int t0 = 0; t0 < nlb; t0 += chunk) {
-      const int t1 = t0 + chunk < nlb ? t0 + chunk : nlb;
+  // one pass over all tiles in chunks: bound sweep, run filter, LB_Keogh, DTW
+  auto sweep = [&](int ch) -> int {
+    for (int t0 = 0; t0 < nlb; t0 += ch) {
+      const int t1 = t0 + ch < nlb ? t0 + ch : nlb;
       CUDA_OK(cudaMemsetAsync(qc, 0, 32, st));
       ph.begin();
       launch_lb(S, Q, lbtiles, t0, t1, bits, enumerate_all, lb_next, ctx->num_sms, st);
@@ -387,6 +426,76 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
       ph.end(DTWJ_PHASE_PAIRS, 1);
     }
     CUDA_OK(cudaGetLastError());
+    return DTWJ_OK;
+  };
+  for (int attempt = 0;; ++attempt) {
+    bool swept = false;
+    if (attempt == 0 && !(flags & DTWJ_F_NO_GRAPH) && nlb > 0) {
+      // the first pass runs as a CUDA graph: replayed if this context captured
+      // the same launches before, captured (then launched) otherwise
+      std::vector<unsigned char> key;
+      auto put = [&key](const void* p, size_t bytes) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        key.insert(key.end(), b, b + bytes);
+      };
+      const int band_cg[2] = {band.C, band.G};
+      const int64_t misc[9] = {nlb, chunk, enumerate_all, masked, ctx->num_sms, ph.on,
+                               (int64_t)ph.used, (int64_t)(uintptr_t)lbtiles,
+                               (int64_t)(uintptr_t)bits};
+      put(&S, sizeof S);
+      put(&Q, sizeof Q);
+      put(band_cg, sizeof band_cg);
+      put(misc, sizeof misc);
+      if (ctx->sweep_exec && key == ctx->sweep_key) {
+        CUDA_OK(cudaGraphLaunch(ctx->sweep_exec, st));
+        for (size_t k = 0; k + 3 < ctx->sweep_marks.size(); k += 4)
+          ph.marks.push_back({ctx->sweep_marks[k], (size_t)ctx->sweep_marks[k + 1],
+                              (size_t)ctx->sweep_marks[k + 2], ctx->sweep_marks[k + 3]});
+        ph.used = ctx->sweep_ev1;
+        swept = true;
+      } else {
+        if (ctx->sweep_exec) cudaGraphExecDestroy(ctx->sweep_exec);
+        ctx->sweep_exec = nullptr;
+        ctx->sweep_key.clear();
+        const size_t u0 = ph.used, m0 = ph.marks.size();
+        // events the capture records must exist before it starts
+        if (ph.on) ph.ev(u0 + 8 * ((size_t)(nlb + chunk - 1) / chunk) + 8);
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+          ph.capturing = true;
+          const int src = sweep(chunk);
+          ph.capturing = false;
+          ok = cudaStreamEndCapture(st, &graph) == cudaSuccess && src == DTWJ_OK && graph;
+        }
+        if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        if (graph) cudaGraphDestroy(graph);
+        if (ok && cudaGraphLaunch(exec, st) == cudaSuccess) {
+          ctx->sweep_exec = exec;
+          ctx->sweep_key = key;
+          ctx->sweep_marks.clear();
+          for (size_t k = m0; k < ph.marks.size(); ++k) {
+            const auto& mk = ph.marks[k];
+            ctx->sweep_marks.insert(ctx->sweep_marks.end(),
+                                    {mk.phase, (int)mk.a, (int)mk.b, mk.launches});
+          }
+          ctx->sweep_ev0 = u0;
+          ctx->sweep_ev1 = ph.used;
+          swept = true;
+        } else {
+          // not capturable here: fall back to direct launches
+          if (exec) cudaGraphExecDestroy(exec);
+          cudaGetLastError();
+          ph.used = u0;
+          ph.marks.resize(m0);
+        }
+      }
+    }
+    if (!swept) {
+      const int src = sweep(chunk);
+      if (src) return src;
+    }
     // a survivor queue that overflowed loses pairs: sweep again in smaller chunks
     int sweep_status = 0;
     CUDA_OK(cudaMemcpyAsync(&sweep_status, S.status, 4, cudaMemcpyDeviceToHost, st));
@@ -524,6 +633,7 @@ void dtwj_ctx_destroy(dtwj_ctx* c) {
   cudaStreamSynchronize(c->stream);
   for (auto& b : c->bufs)
     if (b.p) cudaFree(b.p);
+  if (c->sweep_exec) cudaGraphExecDestroy(c->sweep_exec);
   for (auto e : c->pool) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);

@@ -109,6 +109,7 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
   T last = INF;
   T result = INF;
   *abandoned = false;
+#pragma unroll 2
   for (int tau = 0; tau <= tau_end; ++tau) {
     const int r = tau - g;
     T left = __shfl_up_sync(gm, last, 1, G);

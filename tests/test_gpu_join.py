@@ -46,11 +46,29 @@ def test_flags_do_not_change_the_result(gpu_dtwj, golden):
     c = [g for g in golden if g["name"] == "rw6k_m128_w6"][0]
     base = gpu_dtwj.join(c["series"], c["m"], c["w"])
     for fl in (gpu_dtwj.F_NO_MASKED, gpu_dtwj.F_NO_SEED, gpu_dtwj.F_NO_DIAG,
-               gpu_dtwj.F_NO_SEED | gpu_dtwj.F_NO_MASKED):
+               gpu_dtwj.F_NO_SEED | gpu_dtwj.F_NO_MASKED, gpu_dtwj.F_NO_GRAPH):
         r = gpu_dtwj.join(c["series"], c["m"], c["w"], fl)
         assert (r.i, r.j, r.dist) == (base.i, base.j, base.dist), fl
     nd = gpu_dtwj.join(c["series"], c["m"], c["w"], gpu_dtwj.F_NO_DIAG)
     assert nd.pruned_fast == 0 and nd.pairs == base.pairs
+
+
+def test_graph_replay_matches_direct_launches(gpu_dtwj, golden):
+    # a context captures the sweep as a CUDA graph on the first join and
+    # replays it on the next join of the same shape
+    c = [g for g in golden if g["name"] == "rw20k"][0]
+    x, m, w = c["series"], c["m"], c["w"]
+    with gpu_dtwj.Context() as ctx:
+        first = ctx.join(x, m, w, gpu_dtwj.F_PROFILE)
+        replay = ctx.join(x, m, w, gpu_dtwj.F_PROFILE)
+        direct = ctx.join(x, m, w, gpu_dtwj.F_PROFILE | gpu_dtwj.F_NO_GRAPH)
+        again = ctx.join(x, m, w, gpu_dtwj.F_PROFILE)
+    for r in (first, replay, direct, again):
+        _check(r, c["i"], c["j"], c["dist"], "graph")
+        assert r.pairs == first.pairs and r.pruned_fast == first.pruned_fast
+    diag = gpu_dtwj.PHASES.index("diag")
+    assert replay.phase_launches == first.phase_launches == direct.phase_launches
+    assert replay.phase_seconds[diag] > 0
 
 
 def test_deterministic(gpu_dtwj, golden):
