@@ -58,7 +58,8 @@ extern "C" {
 #define DTWJ_F_NO_MASKED 0x1u   /* skip the masked diagonal bound             */
 #define DTWJ_F_NO_SEED 0x2u     /* no ED-profile seeding of the best-so-far   */
 #define DTWJ_F_NO_DIAG 0x4u     /* skip all diagonal bounds (LB_Keogh + DTW)  */
-#define DTWJ_F_LEARNED 0x8u     /* order the tile queue with the loaded MLP   */
+#define DTWJ_F_LEARNED 0x8u     /* sweep tiles in the order the context's MLP
+                                   scores them (dtwj_ctx_set_model)           */
 #define DTWJ_F_VERBOSE 0x10u    /* phase timings on stderr                    */
 #define DTWJ_F_PROFILE 0x20u    /* per-phase device times (CUDA events)       */
 #define DTWJ_F_NO_GRAPH 0x40u   /* launch the sweep directly, not as a CUDA graph
@@ -150,6 +151,51 @@ int dtwj_pair_dtw(const double* x, int64_t n, int32_t m, int32_t w, const int64_
 int dtwj_pair_dtw_noalloc(const double* x_dev, int64_t n, int32_t m, int32_t w,
                           const int64_t* pi_dev, const int64_t* pj_dev, int64_t count,
                           int32_t precise, double* dist_dev, void* stream);
+
+/* ---- Learned tile ordering (no counterpart in the reference) ----
+ * A small MLP scores each diagonal-sweep tile with a prediction of the
+ * smallest DTW distance among its pairs; with DTWJ_F_LEARNED a context sweeps
+ * the tiles in ascending order of that score so the best-so-far tightens
+ * early.  The score only orders tiles: every pair is still judged by the same
+ * bounds and exact DTW, so the result is that of the plain order.
+ * Network: 64 -> 128 -> 128 -> 1, ReLU, mean squared error, Adam; BF16
+ * weights on the tensor cores with FP32 accumulation and FP32 master weights.
+ * Parameters (FP32, DTWJ_MLP_PARAMS values): W1 [128][64], b1 [128],
+ * W2 [128][128], b2 [128], w3 [128], b3. */
+#define DTWJ_MLP_IN 64
+#define DTWJ_MLP_HIDDEN 128
+#define DTWJ_MLP_PARAMS 24961
+typedef struct dtwj_mlp dtwj_mlp;
+/* He-uniform initial weights from `seed`, zero biases. */
+int dtwj_mlp_create(int device, uint64_t seed, dtwj_mlp** out);
+void dtwj_mlp_destroy(dtwj_mlp* net);
+int dtwj_mlp_get(dtwj_mlp* net, float* params);
+int dtwj_mlp_set(dtwj_mlp* net, const float* params);  /* also resets Adam */
+/* `epochs` passes of Adam over shuffled minibatches of `batch` (<= 8192) rows
+ * of x [count][64] against targets y [count]; *last_loss = the last epoch's
+ * mean squared error. */
+int dtwj_mlp_train(dtwj_mlp* net, const float* x, const float* y, int64_t count,
+                   int32_t epochs, int32_t batch, float lr, uint64_t seed, float* last_loss);
+int dtwj_mlp_predict(dtwj_mlp* net, const float* x, int64_t count, float* out);
+/* Gradient of the mean squared error over one batch (count <= 8192) at the
+ * current parameters, in the parameter layout: BF16 tensor-core path
+ * (precise = 0, the one training uses) or the FP32 debug path (precise = 1). */
+int dtwj_mlp_grad(dtwj_mlp* net, const float* x, const float* y, int64_t count,
+                  int32_t precise, float* grad, float* loss);
+int dtwj_mlp_save(dtwj_mlp* net, const char* path);
+int dtwj_mlp_load(int device, const char* path, dtwj_mlp** out);
+/* The network joins with DTWJ_F_LEARNED use on this context (not owned; it
+ * must live on the context's device and outlive its use; NULL clears). */
+int dtwj_ctx_set_model(dtwj_ctx* ctx, dtwj_mlp* net);
+/* The diagonal-sweep tiles of a series, the units the learned order sorts:
+ * *count = their number; with non-null arrays of *count entries:
+ * desc[4t .. 4t+3] = (first lag, first row, rows, lags of the first row),
+ * features[64t ..] = the tile's 64 features, min_dist[t] = the exact smallest
+ * DTW distance among the tile's pairs (+inf if none).  min_dist needs a sweep
+ * in which every tile prunes only against its own best-so-far: far slower
+ * than a join; it produces the training targets of the network. */
+int dtwj_ctx_tiles(dtwj_ctx* ctx, const double* x, int64_t n, int32_t m, int32_t w,
+                   int64_t* count, int32_t* desc, float* features, double* min_dist);
 
 /* Band from a ratio: ceil(ratio*m) (rounding=0) or the reference's
  * max(round(ratio*m), 1) (rounding=1, GPU_version1/src/AAAA.cu:34). */

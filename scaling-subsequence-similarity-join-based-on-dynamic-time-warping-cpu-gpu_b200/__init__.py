@@ -60,7 +60,22 @@ EXPORTS = (
     "dtwj_band",
     "dtwj_strerror",
     "dtwj_device_count",
+    "dtwj_mlp_create",
+    "dtwj_mlp_destroy",
+    "dtwj_mlp_get",
+    "dtwj_mlp_set",
+    "dtwj_mlp_train",
+    "dtwj_mlp_predict",
+    "dtwj_mlp_grad",
+    "dtwj_mlp_save",
+    "dtwj_mlp_load",
+    "dtwj_ctx_set_model",
+    "dtwj_ctx_tiles",
 )
+
+MLP_IN = 64
+MLP_HIDDEN = 128
+MLP_PARAMS = 24961
 
 
 class DtwjError(RuntimeError):
@@ -159,6 +174,20 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dtwj_strerror.argtypes = [ctypes.c_int]
     lib.dtwj_strerror.restype = ctypes.c_char_p
     lib.dtwj_device_count.argtypes = []
+    f32p = P(ctypes.c_float)
+    lib.dtwj_mlp_create.argtypes = [ctypes.c_int, ctypes.c_uint64, P(vp)]
+    lib.dtwj_mlp_destroy.argtypes = [vp]
+    lib.dtwj_mlp_destroy.restype = None
+    lib.dtwj_mlp_get.argtypes = [vp, f32p]
+    lib.dtwj_mlp_set.argtypes = [vp, f32p]
+    lib.dtwj_mlp_train.argtypes = [vp, f32p, f32p, i64, i32, i32, ctypes.c_float,
+                                   ctypes.c_uint64, f32p]
+    lib.dtwj_mlp_predict.argtypes = [vp, f32p, i64, f32p]
+    lib.dtwj_mlp_grad.argtypes = [vp, f32p, f32p, i64, i32, f32p, f32p]
+    lib.dtwj_mlp_save.argtypes = [vp, ctypes.c_char_p]
+    lib.dtwj_mlp_load.argtypes = [ctypes.c_int, ctypes.c_char_p, P(vp)]
+    lib.dtwj_ctx_set_model.argtypes = [vp, vp]
+    lib.dtwj_ctx_tiles.argtypes = [vp, P(d), i64, i32, i32, P(i64), P(i32), f32p, P(d)]
     _lib = lib
     return lib
 
@@ -243,6 +272,35 @@ class Context:
             raise DtwjError(rc, "dtwj_ctx_join")
         return JoinResult._from(r)
 
+    def set_model(self, net):
+        """Network used by joins with F_LEARNED on this context (None clears)."""
+        rc = load().dtwj_ctx_set_model(self._h, net._h if net is not None else None)
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_set_model")
+        self._model = net  # keep it alive while the context may use it
+
+    def tiles(self, x, m: int, w: int, features: bool = True, min_dist: bool = False):
+        """(desc [T][4] = (first lag, first row, rows, lags), features [T][64] or
+        None, min_dist [T] or None) for the diagonal-sweep tiles of x."""
+        a = _f64(x)
+        cnt = ctypes.c_int64()
+        lib = load()
+        rc = lib.dtwj_ctx_tiles(self._h, _dptr(a), a.size, m, w, ctypes.byref(cnt), None, None,
+                                None)
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_tiles")
+        t = cnt.value
+        desc = np.empty((t, 4), dtype=np.int32)
+        feat = np.empty((t, MLP_IN), dtype=np.float32) if features else None
+        md = np.empty(t, dtype=np.float64) if min_dist else None
+        rc = lib.dtwj_ctx_tiles(self._h, _dptr(a), a.size, m, w, ctypes.byref(cnt),
+                                desc.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                _fptr(feat) if feat is not None else None,
+                                _dptr(md) if md is not None else None)
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_tiles")
+        return desc, feat, md
+
     def join_device(self, dev_ptr: int, n: int, m: int, w: int, flags: int = 0) -> JoinResult:
         """Join a series already in device memory (dev_ptr: n float64)."""
         r = _Result()
@@ -293,3 +351,96 @@ def dtw_motif_discovery(ts, subseqlen: int, maxwarp: int, output_time_file_path:
     with open(output_time_file_path, "a") as f:
         f.write("%f\n" % r.seconds_join)
     return r
+
+
+def _f32(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class MLP:
+    """Tile-scoring network of the learned ordering (dtwj_mlp_*): 64 -> 128 ->
+    128 -> 1, BF16 tensor-core GEMMs with FP32 accumulation, Adam."""
+
+    def __init__(self, device: int = 0, seed: int = 0, _handle=None):
+        if _handle is None:
+            h = ctypes.c_void_p()
+            rc = load().dtwj_mlp_create(device, seed, ctypes.byref(h))
+            if rc != OK:
+                raise DtwjError(rc, "dtwj_mlp_create")
+            _handle = h
+        self._h = _handle
+
+    @classmethod
+    def load_file(cls, path: str, device: int = 0) -> "MLP":
+        h = ctypes.c_void_p()
+        rc = load().dtwj_mlp_load(device, path.encode(), ctypes.byref(h))
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_mlp_load")
+        return cls(_handle=h)
+
+    def close(self):
+        if self._h:
+            load().dtwj_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.empty(MLP_PARAMS, dtype=np.float32)
+        rc = load().dtwj_mlp_get(self._h, _fptr(p))
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_mlp_get")
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = _f32(p)
+        assert p.size == MLP_PARAMS
+        rc = load().dtwj_mlp_set(self._h, _fptr(p))
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_mlp_set")
+
+    def train(self, x, y, epochs: int = 1, batch: int = 4096, lr: float = 1e-3,
+              seed: int = 0) -> float:
+        x = _f32(x).reshape(-1, MLP_IN)
+        y = _f32(y).reshape(-1)
+        loss = ctypes.c_float()
+        rc = load().dtwj_mlp_train(self._h, _fptr(x), _fptr(y), x.shape[0], epochs, batch, lr,
+                                   seed, ctypes.byref(loss))
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_mlp_train")
+        return loss.value
+
+    def predict(self, x) -> np.ndarray:
+        x = _f32(x).reshape(-1, MLP_IN)
+        out = np.empty(x.shape[0], dtype=np.float32)
+        rc = load().dtwj_mlp_predict(self._h, _fptr(x), x.shape[0], _fptr(out))
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_mlp_predict")
+        return out
+
+    def grad(self, x, y, precise: bool = False):
+        """(gradient in the parameter layout, loss) of the mean squared error."""
+        x = _f32(x).reshape(-1, MLP_IN)
+        y = _f32(y).reshape(-1)
+        g = np.empty(MLP_PARAMS, dtype=np.float32)
+        loss = ctypes.c_float()
+        rc = load().dtwj_mlp_grad(self._h, _fptr(x), _fptr(y), x.shape[0], 1 if precise else 0,
+                                  _fptr(g), ctypes.byref(loss))
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_mlp_grad")
+        return g, loss.value
+
+    def save(self, path: str):
+        rc = load().dtwj_mlp_save(self._h, path.encode())
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_mlp_save")

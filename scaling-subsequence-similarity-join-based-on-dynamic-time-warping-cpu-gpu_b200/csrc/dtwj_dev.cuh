@@ -132,6 +132,7 @@ struct DevSearch {
   unsigned int* run_next;
   unsigned int run_cap;
   int2* queue;                  // survivor pairs of the current chunk
+  int* qser;                    // their best-so-far slot (nullptr: the series of i)
   unsigned int* queue_count;
   unsigned int* queue_next;
   unsigned int queue_cap;
@@ -188,8 +189,13 @@ int mask_table_max(int m);
 void launch_mask(const DevSeries& S, unsigned int* counts, int lt_max, double* diff,
                  double* mean_acc, float* zmax, cudaStream_t st);
 // Row minima over partners j >= i + m on LB tiles (lb.cu layout).
+// With tile_best (ntiles entries, 0xffffffff at launch): also each tile's
+// smallest key high bits.
 void launch_mp(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long long* keys,
-               cudaStream_t st);
+               cudaStream_t st, unsigned int* tile_best = nullptr);
+// bsf2[t] = an upper bound on tile t's smallest squared DTW (its ED^2 minimum).
+void launch_tile_bound(const unsigned int* tile_best, int ntiles, unsigned int* bsf2,
+                       cudaStream_t st);
 // Full profile: lo = row minima of the reversed series (nullptr: upper only).
 void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
                         const unsigned long long* lo, double* mp, int64_t* mpi,
@@ -218,6 +224,10 @@ void launch_runs(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int 
                  int tile_end, const unsigned int* bits, bool masked, bool bounds, int num_sms,
                  cudaStream_t st);
 void launch_center(const DevSeries& S, cudaStream_t st);
+// 64 features per tile for the learned ordering (features.cu), from the
+// profile keys of the series' rows; out[64 * t ...] for tile t.
+void launch_tile_features(const DevSeries& S, const Tile* tiles, int ntiles,
+                          const unsigned long long* keys, float* out, cudaStream_t st);
 // LB_Keogh over the candidates the run filter queued in Q.kq; survivors go to
 // Q.queue.
 void launch_keogh(const DevSeries& S, const DevSearch& Q, int num_sms, cudaStream_t st);
@@ -231,6 +241,14 @@ void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
 void launch_verify(const DevSeries& S, const DevSearch& Q, BandShape band, double* out_d2,
                    unsigned long long* best_d2, unsigned long long* best_ij, float* best_f32,
                    cudaStream_t st);
+}  // namespace dtwj
+struct dtwj_mlp;
+namespace dtwj {
+// Tile scores for the learned order (mlp.cu): x_dev [count][64] on the
+// device, after the work queued on st; y_dev [count].
+int mlp_predict_device(dtwj_mlp* net, const float* x_dev, int64_t count, float* y_dev,
+                       cudaStream_t st);
+int mlp_device(const dtwj_mlp* net);
 void launch_pair_dtw(const DevSeries& S, const int2* pairs, int count, bool precise,
                      BandShape band, double* out_d2, cudaStream_t st);
 

@@ -58,6 +58,8 @@ struct dtwj_ctx {
   std::vector<Tile> lbtiles_host;    // kLbLags-lag tiles of the diagonal sweep
   int64_t lbtiles_n = -1, lbtiles_m = -1;  // single-series shape the tiles were built for
   std::vector<unsigned int> host_u32;      // staging of small host -> device copies
+  std::vector<Tile> tiles_run;             // the tiles in the order of the current call
+  dtwj_mlp* model = nullptr;               // scores tiles for DTWJ_F_LEARNED (not owned)
   std::vector<cudaEvent_t> pool;  // events for per-phase device times
   // the sweep's launches captured as a CUDA graph, replayed while every
   // launch argument is unchanged (same buffers, tiles, band, flags)
@@ -75,7 +77,7 @@ enum BufId {
   B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
   B_MP, B_MPI, B_CB, B_AF, B_ULF, B_BITS, B_LBTILES, B_KQ, B_SBEG, B_SID, B_SEEDBSF,
-  B_BEST_IJ, B_BEST_F32,
+  B_BEST_IJ, B_BEST_F32, B_QSER, B_TILEBEST, B_FEAT, B_SCORE,
   B_COUNT_
 };
 
@@ -307,17 +309,30 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
 
 int effective_band(int m, int w) { return w > m - 1 ? m - 1 : w; }
 
+// Per-tile outputs of dtwj_ctx_tiles (host arrays, one entry per tile).
+struct TileQuery {
+  float* features;   // [tiles][64] or nullptr
+  double* min_dist;  // exact smallest DTW distance per tile, or nullptr
+};
+
 // Joins one series (sbeg == nullptr, nseries == 1) or a batch of nseries
 // series of one (m, w) stored back to back (series r on samples
 // [sbeg[r], sbeg[r + 1])); outs[r] receives series r's top-1 pair with
-// indices relative to its own first sample.
+// indices relative to its own first sample.  With tq (one series) the call
+// reports per-tile values instead of a join: the tile features, and with
+// tq->min_dist the exact smallest DTW distance of every tile, found by a sweep
+// in which every tile prunes against its own best-so-far only.
 int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg, int nseries,
-             int32_t m, int32_t w_in, uint32_t flags, dtwj_result* outs, double t_upload) {
+             int32_t m, int32_t w_in, uint32_t flags, dtwj_result* outs, double t_upload,
+             const TileQuery* tq = nullptr) {
   Timer wall;
   const int w = effective_band(m, w_in);
   BandShape band;
   if (!choose_band(w, &band)) return DTWJ_ERR_BAND;
-  if (flags & DTWJ_F_LEARNED) return DTWJ_ERR_NOMODEL;
+  const bool learned = (flags & DTWJ_F_LEARNED) && !tq;
+  if (learned && !ctx->model) return DTWJ_ERR_NOMODEL;
+  if (learned && mlp_device(ctx->model) != ctx->device) return DTWJ_ERR_ARG;
+  const bool tile_mode = tq && tq->min_dist;
   const bool masked = !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
   const bool verbose = flags & DTWJ_F_VERBOSE;
   cudaStream_t st = ctx->stream;
@@ -330,10 +345,17 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
 
   build_lb_tiles(ctx, n, m, sbeg, nseries);
   const int nlb = (int)ctx->lbtiles_host.size();
+  // best-so-far slots: one per series, or one per tile for the tile minima
+  const int nslots = tile_mode ? (nlb > 0 ? nlb : 1) : nseries;
+  S.nseries = nslots;
+  std::vector<Tile>& th = ctx->tiles_run;
+  th = ctx->lbtiles_host;
+  if (tile_mode)
+    for (int t = 0; t < nlb; ++t) th[t].series = t;
   Tile* lbtiles;
   ENSURE(B_LBTILES, (size_t)(nlb > 0 ? nlb : 1) * sizeof(Tile), lbtiles);
   if (nlb > 0)
-    CUDA_OK(cudaMemcpyAsync(lbtiles, ctx->lbtiles_host.data(), (size_t)nlb * sizeof(Tile),
+    CUDA_OK(cudaMemcpyAsync(lbtiles, th.data(), (size_t)nlb * sizeof(Tile),
                             cudaMemcpyHostToDevice, st));
 
   // search state
@@ -360,26 +382,76 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   Q.kq_cap = qcap * 2;
   Q.runs = nullptr;
   Q.run_cap = 0;
-  ENSURE(B_BSF2, (size_t)nseries * 4, Q.bsf2);
+  ENSURE(B_BSF2, (size_t)nslots * 4, Q.bsf2);
   ENSURE(B_COUNTERS, kNumCounters * 8, Q.counters);
-  ENSURE(B_CAND, (size_t)kCandCap * sizeof(Candidate), Q.cand);
+  // the tile minima keep a few candidates per tile
+  const unsigned int cand_cap =
+      tile_mode && 16u * (unsigned int)nlb > kCandCap ? 16u * (unsigned int)nlb : kCandCap;
+  ENSURE(B_CAND, (size_t)cand_cap * sizeof(Candidate), Q.cand);
   ENSURE(B_CCOUNT, 4, Q.cand_count);
-  Q.cand_cap = kCandCap;
+  Q.cand_cap = cand_cap;
+  if (tile_mode) ENSURE(B_QSER, (size_t)qcap * sizeof(int), Q.qser);
   CUDA_OK(cudaMemsetAsync(Q.counters, 0, kNumCounters * 8, st));
   CUDA_OK(cudaMemsetAsync(Q.cand_count, 0, 4, st));
-  ctx->host_u32.assign((size_t)nseries + 1, 0x7f800000u);  // +inf per series
-  CUDA_OK(cudaMemcpyAsync(Q.bsf2, ctx->host_u32.data(), (size_t)nseries * 4,
+  ctx->host_u32.assign((size_t)nslots + 1, 0x7f800000u);  // +inf per slot
+  CUDA_OK(cudaMemcpyAsync(Q.bsf2, ctx->host_u32.data(), (size_t)nslots * 4,
                           cudaMemcpyHostToDevice, st));
   unsigned int* seed_bsf;
-  ENSURE(B_SEEDBSF, (size_t)nseries * 4, seed_bsf);
+  ENSURE(B_SEEDBSF, (size_t)nslots * 4, seed_bsf);
+
+  // ---- ED matrix profile (row minima; per tile for the tile minima) ----
+  const bool want_features = learned || (tq && tq->features);
+  unsigned long long* keys = nullptr;
+  if (nlb > 0 && (tile_mode || want_features || !(flags & DTWJ_F_NO_SEED))) {
+    ENSURE(B_KEYS_UP, S.s * 8, keys);
+    unsigned int* tbest = nullptr;
+    if (tile_mode) {
+      ENSURE(B_TILEBEST, (size_t)nlb * 4, tbest);
+      CUDA_OK(cudaMemsetAsync(tbest, 0xff, (size_t)nlb * 4, st));
+    }
+    ph.begin();
+    launch_mp(S, lbtiles, nlb, keys, st, tbest);
+    if (tile_mode) launch_tile_bound(tbest, nlb, Q.bsf2, st);
+    ph.end(DTWJ_PHASE_PROFILE, 2);
+  }
+  // ---- tile features; the learned order sorts the tiles by their score ----
+  if (want_features && nlb > 0) {
+    float* feat;
+    ENSURE(B_FEAT, (size_t)nlb * DTWJ_MLP_IN * 4, feat);
+    launch_tile_features(S, lbtiles, nlb, keys, feat, st);
+    if (tq && tq->features)
+      CUDA_OK(cudaMemcpyAsync(tq->features, feat, (size_t)nlb * DTWJ_MLP_IN * 4,
+                              cudaMemcpyDeviceToHost, st));
+    if (learned) {
+      float* score;
+      ENSURE(B_SCORE, (size_t)nlb * 4, score);
+      rc = mlp_predict_device(ctx->model, feat, nlb, score, st);
+      if (rc) return rc;
+      std::vector<float> sc((size_t)nlb);
+      CUDA_OK(cudaMemcpy(sc.data(), score, (size_t)nlb * 4, cudaMemcpyDeviceToHost));
+      std::vector<int> ord((size_t)nlb);
+      for (int t = 0; t < nlb; ++t) ord[t] = t;
+      // ascending predicted minimum; ties (and NaN scores, last) keep the plain order
+      std::stable_sort(ord.begin(), ord.end(), [&sc](int a, int b) {
+        const bool na = !(sc[a] == sc[a]), nb = !(sc[b] == sc[b]);
+        if (na != nb) return nb;
+        return !na && sc[a] < sc[b];
+      });
+      for (int t = 0; t < nlb; ++t) {
+        th[t] = ctx->lbtiles_host[ord[t]];
+        th[t].order = t;
+      }
+      CUDA_OK(cudaMemcpyAsync(lbtiles, th.data(), (size_t)nlb * sizeof(Tile),
+                              cudaMemcpyHostToDevice, st));
+    }
+  }
+  if (tq && !tile_mode) {
+    CUDA_OK(cudaStreamSynchronize(st));
+    return DTWJ_OK;
+  }
 
   // ---- ED profile seeds ----
-  if (!(flags & DTWJ_F_NO_SEED) && nlb > 0) {
-    unsigned long long* keys;
-    ENSURE(B_KEYS_UP, S.s * 8, keys);
-    ph.begin();
-    launch_mp(S, lbtiles, nlb, keys, st);
-    ph.end(DTWJ_PHASE_PROFILE, 2);
+  if (!tile_mode && !(flags & DTWJ_F_NO_SEED) && nlb > 0) {
     int2* seeds;
     unsigned int* nseeds;  // [nseries] counts, total slots, work counter
     ENSURE(B_SEEDS, (size_t)nseries * kSeeds * sizeof(int2), seeds);
@@ -391,12 +463,13 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
     ph.begin();
     launch_seed_select(S, keys, seeds, nseeds, Q.bsf2, st);
     DevSearch Qs = Q;
+    Qs.qser = nullptr;
     Qs.queue_next = nseeds + nseries + 1;
     Qs.queue_cap = (unsigned int)(nseries * kSeeds);
     launch_pairs(S, Qs, seeds, nseeds + nseries, false, band, ctx->num_sms, st);
     ph.end(DTWJ_PHASE_SEEDS, 2);
   }
-  CUDA_OK(cudaMemcpyAsync(seed_bsf, Q.bsf2, (size_t)nseries * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_OK(cudaMemcpyAsync(seed_bsf, Q.bsf2, (size_t)nslots * 4, cudaMemcpyDeviceToDevice, st));
 
   // ---- diagonal sweep in chunks of LB tiles ----
   const bool enumerate_all = flags & DTWJ_F_NO_DIAG;
@@ -512,31 +585,39 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   ENSURE(B_VERIFY, (size_t)kCandCap * 8, vd2);
   unsigned long long *best_d2, *best_ij;
   float* best_f32;
-  ENSURE(B_BEST, (size_t)nseries * 8, best_d2);
-  ENSURE(B_BEST_IJ, (size_t)nseries * 8, best_ij);
-  ENSURE(B_BEST_F32, (size_t)nseries * 4, best_f32);
+  ENSURE(B_BEST, (size_t)nslots * 8, best_d2);
+  ENSURE(B_BEST_IJ, (size_t)nslots * 8, best_ij);
+  ENSURE(B_BEST_F32, (size_t)nslots * 4, best_f32);
   ph.begin();
   launch_verify(S, Q, band, vd2, best_d2, best_ij, best_f32, st);
   ph.end(DTWJ_PHASE_VERIFY, 4);
   CUDA_OK(cudaEventRecord(ctx->ev1, st));
 
-  std::vector<unsigned long long> d2_h(nseries), ij_h(nseries);
-  std::vector<unsigned int> f32_h(nseries), seed_h(nseries);
+  std::vector<unsigned long long> d2_h(nslots), ij_h(nslots);
+  std::vector<unsigned int> f32_h(nslots), seed_h(nslots);
   unsigned long long cnt_h[kNumCounters];
   unsigned int cand_h = 0;
   int status_h = 0;
-  CUDA_OK(cudaMemcpyAsync(d2_h.data(), best_d2, (size_t)nseries * 8, cudaMemcpyDeviceToHost, st));
-  CUDA_OK(cudaMemcpyAsync(ij_h.data(), best_ij, (size_t)nseries * 8, cudaMemcpyDeviceToHost, st));
-  CUDA_OK(cudaMemcpyAsync(f32_h.data(), best_f32, (size_t)nseries * 4, cudaMemcpyDeviceToHost, st));
-  CUDA_OK(cudaMemcpyAsync(seed_h.data(), seed_bsf, (size_t)nseries * 4, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(d2_h.data(), best_d2, (size_t)nslots * 8, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(ij_h.data(), best_ij, (size_t)nslots * 8, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(f32_h.data(), best_f32, (size_t)nslots * 4, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(cudaMemcpyAsync(seed_h.data(), seed_bsf, (size_t)nslots * 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaMemcpyAsync(cnt_h, Q.counters, sizeof cnt_h, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaMemcpyAsync(&cand_h, Q.cand_count, 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaMemcpyAsync(&status_h, S.status, 4, cudaMemcpyDeviceToHost, st));
   CUDA_OK(cudaStreamSynchronize(st));
   if (status_h & 2) return DTWJ_ERR_OVERFLOW;
-  if (cand_h > kCandCap) return DTWJ_ERR_OVERFLOW;
+  if (cand_h > cand_cap) return DTWJ_ERR_OVERFLOW;
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  if (tile_mode) {
+    for (int t = 0; t < nlb; ++t) {
+      double d2;
+      memcpy(&d2, &d2_h[t], 8);
+      tq->min_dist[t] = d2_h[t] != ~0ull ? std::sqrt(d2) : INFINITY;
+    }
+    return DTWJ_OK;
+  }
 
   for (int r = 0; r < nseries; ++r) {
     dtwj_result* out = &outs[r];
@@ -648,6 +729,50 @@ int dtwj_ctx_join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t 
   if (rc) return rc;
   cudaSetDevice(ctx->device);
   return join_device(ctx, x_dev, n, m, w, flags, out, 0.0);
+}
+
+int dtwj_ctx_set_model(dtwj_ctx* ctx, dtwj_mlp* net) {
+  if (!ctx) return DTWJ_ERR_ARG;
+  if (net && mlp_device(net) != ctx->device) return DTWJ_ERR_ARG;
+  ctx->model = net;
+  return DTWJ_OK;
+}
+
+int dtwj_ctx_tiles(dtwj_ctx* ctx, const double* x, int64_t n, int32_t m, int32_t w,
+                   int64_t* count, int32_t* desc, float* features, double* min_dist) {
+  if (!ctx || !count) return DTWJ_ERR_ARG;
+  int rc = check_args(x, n, m, w);
+  if (rc) return rc;
+  cudaSetDevice(ctx->device);
+  build_lb_tiles(ctx, n, m, nullptr, 1);
+  const int64_t nt = (int64_t)ctx->lbtiles_host.size();
+  *count = nt;
+  if (desc) {
+    const int64_t s = n - m + 1;
+    for (int64_t t = 0; t < nt; ++t) {
+      const Tile& T = ctx->lbtiles_host[t];
+      const int64_t lags = s - T.i0 - T.L0 < kLbLags ? s - T.i0 - T.L0 : kLbLags;
+      desc[4 * t] = T.L0;
+      desc[4 * t + 1] = T.i0;
+      desc[4 * t + 2] = T.rows;
+      desc[4 * t + 3] = (int32_t)lags;
+    }
+  }
+  if (!features && !min_dist) return DTWJ_OK;
+  double* dev = nullptr;
+  rc = upload(ctx, x, n, &dev);
+  if (rc) return rc;
+  TileQuery tq;
+  tq.features = features;
+  tq.min_dist = min_dist;
+  if (min_dist && features) {
+    // features first (a plain pass), then the minima sweep
+    TileQuery f1 = {features, nullptr};
+    rc = run_join(ctx, dev, n, nullptr, 1, m, w, 0, nullptr, 0.0, &f1);
+    if (rc) return rc;
+    tq.features = nullptr;
+  }
+  return run_join(ctx, dev, n, nullptr, 1, m, w, DTWJ_F_NO_GRAPH, nullptr, 0.0, &tq);
 }
 
 int dtwj_ctx_join(dtwj_ctx* ctx, const double* x, int64_t n, int32_t m, int32_t w,

@@ -43,7 +43,8 @@ struct MpShared {
 };
 
 __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* tiles,
-                                                      unsigned long long* keys) {
+                                                      unsigned long long* keys,
+                                                      unsigned int* tile_best, int tile_base) {
   extern __shared__ __align__(16) unsigned char smraw[];
   MpShared& sh = *reinterpret_cast<MpShared*>(smraw);
   const Tile T = tiles[blockIdx.x];
@@ -149,10 +150,32 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
     }
   }
   __syncthreads();
+  unsigned int tmin = 0xffffffffu;  // the tile's smallest key (high bits of ED^2)
   for (int x = t; x < T.rows; x += kLbThreads) {
     const unsigned long long v = sh.rowbest[x];
-    if (v != ULLONG_MAX) atomicMin(&keys[i0 + x], v);
+    if (v != ULLONG_MAX) {
+      atomicMin(&keys[i0 + x], v);
+      tmin = min(tmin, (unsigned int)(v >> 32));
+    }
   }
+  if (tile_best) {
+    for (int o = 16; o > 0; o >>= 1) tmin = min(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+    if (lane == 0 && tmin != 0xffffffffu) atomicMin(&tile_best[tile_base + blockIdx.x], tmin);
+  }
+}
+
+// Per tile, an upper bound on its smallest squared DTW distance: the ED^2 of
+// its closest pair (ED >= DTW), from the truncated key rounded up.
+__global__ void k_tile_bound(const unsigned int* tile_best, int ntiles, unsigned int* bsf2) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  const unsigned int hi = tile_best[t];
+  if (hi == 0xffffffffu) {
+    bsf2[t] = 0x7f800000u;
+    return;
+  }
+  const unsigned long long bits = ((unsigned long long)hi + 1ull) << 32;
+  bsf2[t] = __float_as_uint(__double2float_ru(__longlong_as_double((long long)bits)));
 }
 
 __global__ void k_fill_u64(unsigned long long* p, int64_t n, unsigned long long v) {
@@ -298,8 +321,13 @@ void launch_reverse(const double* a, int64_t n, double* out, cudaStream_t st) {
   k_reverse<<<1024, 256, 0, st>>>(a, n, out);
 }
 
+void launch_tile_bound(const unsigned int* tile_best, int ntiles, unsigned int* bsf2,
+                       cudaStream_t st) {
+  if (ntiles > 0) k_tile_bound<<<(ntiles + 255) / 256, 256, 0, st>>>(tile_best, ntiles, bsf2);
+}
+
 void launch_mp(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long long* keys,
-               cudaStream_t st) {
+               cudaStream_t st, unsigned int* tile_best) {
   k_fill_u64<<<1024, 256, 0, st>>>(keys, S.s, ULLONG_MAX);
   if (ntiles <= 0) return;
   static bool configured = false;
@@ -310,7 +338,7 @@ void launch_mp(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long 
   const int slab = 1 << 20;
   for (int b = 0; b < ntiles; b += slab) {
     const int cnt = ntiles - b < slab ? ntiles - b : slab;
-    k_mp<<<cnt, kLbThreads, sizeof(MpShared), st>>>(S, tiles + b, keys);
+    k_mp<<<cnt, kLbThreads, sizeof(MpShared), st>>>(S, tiles + b, keys, tile_best, b);
   }
 }
 

@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
     const int2 pr = pairs[idx];
     if (pr.x < 0) continue;  // an unused seed slot
     const int64_t i = pr.x, j = pr.y;
-    const int sr = series_of(S, i);
+    const int sr = Q.qser ? Q.qser[idx] : series_of(S, i);
     unsigned int* bsf2 = Q.bsf2 + sr;
     const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
     float thr = prune_threshold_now(bsf2, S.m);

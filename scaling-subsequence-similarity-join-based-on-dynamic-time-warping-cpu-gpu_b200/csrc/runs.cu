@@ -256,8 +256,12 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch 
       // no bounds: every pair of the run goes to the DTW stage
       for (int p = lane; p < len; p += 32) {
         const unsigned int slot = atomicAdd(Q.queue_count, 1u);
-        if (slot < Q.queue_cap) Q.queue[slot] = make_int2((int)(i0 + p), (int)(j0 + p));
-        else atomicOr(S.status, 2);
+        if (slot < Q.queue_cap) {
+          Q.queue[slot] = make_int2((int)(i0 + p), (int)(j0 + p));
+          if (Q.qser) Q.qser[slot] = T.series;
+        } else {
+          atomicOr(S.status, 2);
+        }
       }
       continue;
     }
@@ -422,8 +426,12 @@ __global__ void __launch_bounds__(kKeoghWarps * 32, 5) k_keogh(DevSeries S, DevS
           ++pruned;
         } else {
           const unsigned int slot = atomicAdd(Q.queue_count, 1u);
-          if (slot < Q.queue_cap) Q.queue[slot] = make_int2((int)wi.x, (int)wj.x);
-          else atomicOr(S.status, 2);
+          if (slot < Q.queue_cap) {
+            Q.queue[slot] = make_int2((int)wi.x, (int)wj.x);
+            if (Q.qser) Q.qser[slot] = serv[warp][e];
+          } else {
+            atomicOr(S.status, 2);
+          }
         }
       }
     }
