@@ -197,6 +197,20 @@ int dtwj_ctx_set_model(dtwj_ctx* ctx, dtwj_mlp* net);
 int dtwj_ctx_tiles(dtwj_ctx* ctx, const double* x, int64_t n, int32_t m, int32_t w,
                    int64_t* count, int32_t* desc, float* features, double* min_dist);
 
+/* ---- Autotuning of the DTW band layout (no counterpart in the reference;
+ * the reference fixes its layout at compile time with REGISTER_NUM) ----
+ * The banded DTW runs a group of G lanes per pair with C band cells per lane
+ * (C * G >= 2w + 1).  Every layout computes the same distances, so the choice
+ * only changes speed.  dtwj_band_shapes lists the layouts tried for band w
+ * (returns how many; writes up to max); dtwj_time_band measures one of them
+ * on exact FP32 DTW of `pairs` window pairs of a seeded random walk (band
+ * cells per second); dtwj_ctx_set_band makes a context's joins use layout
+ * (C, G) for band w (0, 0: back to the default choice). */
+int dtwj_band_shapes(int32_t w, int32_t* C, int32_t* G, int32_t max);
+int dtwj_time_band(int device, int32_t m, int32_t w, int32_t C, int32_t G, int32_t pairs,
+                   double* cells_per_s);
+int dtwj_ctx_set_band(dtwj_ctx* ctx, int32_t w, int32_t C, int32_t G);
+
 /* Band from a ratio: ceil(ratio*m) (rounding=0) or the reference's
  * max(round(ratio*m), 1) (rounding=1, GPU_version1/src/AAAA.cu:34). */
 int32_t dtwj_band(int32_t m, double ratio, int32_t rounding);

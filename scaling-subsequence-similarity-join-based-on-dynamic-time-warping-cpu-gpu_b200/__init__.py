@@ -71,6 +71,9 @@ EXPORTS = (
     "dtwj_mlp_load",
     "dtwj_ctx_set_model",
     "dtwj_ctx_tiles",
+    "dtwj_band_shapes",
+    "dtwj_time_band",
+    "dtwj_ctx_set_band",
 )
 
 MLP_IN = 64
@@ -187,6 +190,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dtwj_mlp_save.argtypes = [vp, ctypes.c_char_p]
     lib.dtwj_mlp_load.argtypes = [ctypes.c_int, ctypes.c_char_p, P(vp)]
     lib.dtwj_ctx_set_model.argtypes = [vp, vp]
+    lib.dtwj_band_shapes.argtypes = [i32, P(i32), P(i32), i32]
+    lib.dtwj_time_band.argtypes = [ctypes.c_int, i32, i32, i32, i32, i32, P(d)]
+    lib.dtwj_ctx_set_band.argtypes = [vp, i32, i32, i32]
     lib.dtwj_ctx_tiles.argtypes = [vp, P(d), i64, i32, i32, P(i64), P(i32), f32p, P(d)]
     _lib = lib
     return lib
@@ -271,6 +277,13 @@ class Context:
         if rc != OK:
             raise DtwjError(rc, "dtwj_ctx_join")
         return JoinResult._from(r)
+
+    def set_band(self, w: int, C: int = 0, G: int = 0):
+        """Joins with band w use the DTW layout (C cells per lane, G lanes per
+        pair); (0, 0) restores the default choice."""
+        rc = load().dtwj_ctx_set_band(self._h, w, C, G)
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_set_band")
 
     def set_model(self, net):
         """Network used by joins with F_LEARNED on this context (None clears)."""
@@ -444,3 +457,22 @@ class MLP:
         rc = load().dtwj_mlp_save(self._h, path.encode())
         if rc != OK:
             raise DtwjError(rc, "dtwj_mlp_save")
+
+
+def band_shapes(w: int) -> list:
+    """[(C, G), ...]: the DTW layouts the autotuner tries for band w."""
+    C = (ctypes.c_int32 * 16)()
+    G = (ctypes.c_int32 * 16)()
+    k = load().dtwj_band_shapes(w, C, G, 16)
+    if k < 0:
+        raise DtwjError(k, "dtwj_band_shapes")
+    return [(C[q], G[q]) for q in range(min(k, 16))]
+
+
+def time_band(m: int, w: int, C: int, G: int, pairs: int = 2048, device: int = 0) -> float:
+    """Band cells per second of exact FP32 DTW with layout (C, G)."""
+    v = ctypes.c_double()
+    rc = load().dtwj_time_band(device, m, w, C, G, pairs, ctypes.byref(v))
+    if rc != OK:
+        raise DtwjError(rc, "dtwj_time_band")
+    return v.value

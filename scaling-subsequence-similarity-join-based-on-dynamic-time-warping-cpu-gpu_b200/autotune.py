@@ -1,0 +1,64 @@
+"""Autotuner of the DTW band layout, keyed by (m, w), with a JSON cache.
+
+The banded DTW runs G lanes per pair with C band cells per lane; every layout
+that covers the band computes the same distances, so the choice is only about
+speed.  `tune` times each candidate (band cells per second on exact FP32 DTW
+of random-walk window pairs, dtwj_time_band) and keeps the fastest; results
+are cached in a JSON file:
+
+    {"m=1024,w=52": {"C": 7, "G": 16, "cells_per_s": ..., "tried": [[C, G, cells_per_s], ...]}}
+
+`apply` sets the cached layout on a context (dtwj_ctx_set_band).
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+if __package__:
+    from . import band_shapes, time_band
+else:  # loaded by path
+    _pkg = sys.modules.get("dtwj")
+    band_shapes, time_band = _pkg.band_shapes, _pkg.time_band
+
+
+def _key(m: int, w: int) -> str:
+    return "m=%d,w=%d" % (m, w)
+
+
+def load_cache(path: str) -> dict:
+    if path and os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def tune(m: int, w: int, cache_path: str | None = None, pairs: int = 2048, timer=None,
+         shapes=None) -> dict:
+    """Best layout for (m, w): from the cache if present, else measured (and
+    written back to the cache).  `timer(m, w, C, G, pairs)` and `shapes(w)`
+    default to the library's measurement and candidate list."""
+    cache = load_cache(cache_path)
+    k = _key(m, w)
+    if k in cache:
+        return cache[k]
+    timer = timer or (lambda m_, w_, C, G, p: time_band(m_, w_, C, G, p))
+    cands = (shapes or band_shapes)(min(w, m - 1))
+    tried = [[C, G, float(timer(m, w, C, G, pairs))] for C, G in cands]
+    C, G, best = max(tried, key=lambda t: t[2])
+    entry = {"C": C, "G": G, "cells_per_s": best, "tried": tried}
+    if cache_path:
+        cache[k] = entry
+        tmp = cache_path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+        os.replace(tmp, cache_path)
+    return entry
+
+
+def apply(ctx, m: int, w: int, cache_path: str | None = None, **kw) -> dict:
+    """Tune (or read the cache for) (m, w) and set the layout on `ctx`."""
+    e = tune(m, w, cache_path, **kw)
+    ctx.set_band(min(w, m - 1), e["C"], e["G"])
+    return e

@@ -177,6 +177,11 @@ struct BandShape {
 // Picks lanes-per-pair G in {4, 8, 16, 32} and cells-per-lane C in [2, 16]
 // covering 2w+1 diagonals with the least waste.  Returns false if w > 255.
 bool choose_band(int w, BandShape* out);
+// (C, G) has a kernel instantiation and covers band w.
+bool band_shape_ok(int w, int C, int G);
+// The shapes the autotuner tries for band w (per G the two smallest covering
+// C); writes up to max, returns how many there are.
+int band_shapes(int w, BandShape* out, int max);
 
 // ---- launches (all on `stream`) ----
 void launch_check_finite(const double* a, int64_t n, int* status, cudaStream_t st);

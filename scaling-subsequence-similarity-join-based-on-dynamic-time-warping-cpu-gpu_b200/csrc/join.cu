@@ -60,6 +60,7 @@ struct dtwj_ctx {
   std::vector<unsigned int> host_u32;      // staging of small host -> device copies
   std::vector<Tile> tiles_run;             // the tiles in the order of the current call
   dtwj_mlp* model = nullptr;               // scores tiles for DTWJ_F_LEARNED (not owned)
+  std::vector<std::pair<int, BandShape>> band_override;  // band w -> DTW layout (autotuner)
   std::vector<cudaEvent_t> pool;  // events for per-phase device times
   // the sweep's launches captured as a CUDA graph, replayed while every
   // launch argument is unchanged (same buffers, tiles, band, flags)
@@ -329,6 +330,8 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   const int w = effective_band(m, w_in);
   BandShape band;
   if (!choose_band(w, &band)) return DTWJ_ERR_BAND;
+  for (const auto& bo : ctx->band_override)
+    if (bo.first == w) band = bo.second;
   const bool learned = (flags & DTWJ_F_LEARNED) && !tq;
   if (learned && !ctx->model) return DTWJ_ERR_NOMODEL;
   if (learned && mlp_device(ctx->model) != ctx->device) return DTWJ_ERR_ARG;
@@ -729,6 +732,90 @@ int dtwj_ctx_join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t 
   if (rc) return rc;
   cudaSetDevice(ctx->device);
   return join_device(ctx, x_dev, n, m, w, flags, out, 0.0);
+}
+
+int dtwj_band_shapes(int32_t w, int32_t* C, int32_t* G, int32_t max) {
+  if (w < 0 || max < 0 || (max > 0 && (!C || !G))) return DTWJ_ERR_ARG;
+  BandShape b[16];
+  const int k = band_shapes(w, b, 16);
+  for (int q = 0; q < k && q < max && q < 16; ++q) {
+    C[q] = b[q].C;
+    G[q] = b[q].G;
+  }
+  return k;
+}
+
+int dtwj_ctx_set_band(dtwj_ctx* ctx, int32_t w, int32_t C, int32_t G) {
+  if (!ctx || w < 0) return DTWJ_ERR_ARG;
+  auto& v = ctx->band_override;
+  for (size_t q = 0; q < v.size(); ++q)
+    if (v[q].first == w) {
+      v.erase(v.begin() + q);
+      break;
+    }
+  if (C == 0 && G == 0) return DTWJ_OK;
+  if (!band_shape_ok(w, C, G)) return DTWJ_ERR_BAND;
+  v.push_back({w, BandShape{C, G}});
+  return DTWJ_OK;
+}
+
+int dtwj_time_band(int device, int32_t m, int32_t w, int32_t C, int32_t G, int32_t pairs,
+                   double* cells_per_s) {
+  if (!cells_per_s || m < 8 || m > DTWJ_MAX_M || w < 0 || pairs < 1) return DTWJ_ERR_ARG;
+  const int we = effective_band(m, w);
+  if (!band_shape_ok(we, C, G)) return DTWJ_ERR_BAND;
+  dtwj_ctx* ctx = nullptr;
+  int rc = dtwj_ctx_create(device, &ctx);
+  if (rc) return rc;
+  do {
+    // a seeded random walk of 8m samples, pairs of windows drawn from it
+    const int64_t n = 8 * (int64_t)m;
+    std::vector<double> x((size_t)n);
+    uint64_t st = 0x9e3779b97f4a7c15ull;
+    double v = 0.0;
+    for (int64_t p = 0; p < n; ++p) {
+      st = st * 6364136223846793005ull + 1442695040888963407ull;
+      v += ((double)(st >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
+      x[(size_t)p] = v;
+    }
+    double* dev = nullptr;
+    if ((rc = upload(ctx, x.data(), n, &dev))) break;
+    DevSeries S;
+    if ((rc = prepare(ctx, dev, n, m, we, false, nullptr, 1, &S))) break;
+    std::vector<int2> pr((size_t)pairs);
+    const int64_t s = n - m + 1;
+    for (int q = 0; q < pairs; ++q) {
+      st = st * 6364136223846793005ull + 1442695040888963407ull;
+      const int a = (int)((st >> 33) % (uint64_t)(s - m));
+      st = st * 6364136223846793005ull + 1442695040888963407ull;
+      const int b = a + m + (int)((st >> 33) % (uint64_t)(s - m - a));
+      pr[(size_t)q] = make_int2(a, b);
+    }
+    int2* dp;
+    double* out;
+    if ((rc = ensure(ctx, B_PAIRS, (size_t)pairs * sizeof(int2), (void**)&dp))) break;
+    if ((rc = ensure(ctx, B_OUT, (size_t)pairs * 8, (void**)&out))) break;
+    if (cudaMemcpyAsync(dp, pr.data(), (size_t)pairs * sizeof(int2), cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess) {
+      rc = DTWJ_ERR_CUDA;
+      break;
+    }
+    const BandShape b = {C, G};
+    launch_pair_dtw(S, dp, pairs, false, b, out, ctx->stream);  // warm-up
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    for (int r = 0; r < 3; ++r) launch_pair_dtw(S, dp, pairs, false, b, out, ctx->stream);
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+      rc = DTWJ_ERR_CUDA;
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    const double cells = 3.0 * pairs * ((double)m * (2 * we + 1) - (double)we * (we + 1));
+    *cells_per_s = ms > 0 ? cells / (ms * 1e-3) : 0.0;
+  } while (0);
+  dtwj_ctx_destroy(ctx);
+  return rc;
 }
 
 int dtwj_ctx_set_model(dtwj_ctx* ctx, dtwj_mlp* net) {

@@ -498,6 +498,27 @@ bool band_supported(int C, int G) {
 
 }  // namespace
 
+bool band_shape_ok(int w, int C, int G) {
+  return w >= 0 && band_supported(C, G) && C * G >= 2 * w + 1;
+}
+
+int band_shapes(int w, BandShape* out, int max) {
+  // per G, the smallest supported C covering the band and the next one up
+  int k = 0;
+  const int Gs[4] = {4, 8, 16, 32};
+  for (int gi = 0; gi < 4; ++gi) {
+    const int G = Gs[gi];
+    int found = 0;
+    for (int C = 2; C <= 16 && found < 2; ++C) {
+      if (!band_shape_ok(w, C, G)) continue;
+      if (k < max) out[k] = {C, G};
+      ++k;
+      ++found;
+    }
+  }
+  return k;
+}
+
 bool choose_band(int w, BandShape* out) {
   const int cells = 2 * w + 1;
   const int Gs[4] = {32, 16, 8, 4};

@@ -197,3 +197,31 @@ def test_context_reuse_leaves_no_stale_state(gpu_dtwj, oracle, synth):
             later = r.pruned_masked + r.pruned_kim + r.pruned_keogh + r.dtw_calls
             assert later <= r.pairs - r.pruned_fast + 2 * 100, (later, r.pairs - r.pruned_fast)
             assert 0 <= r.i < r.j < x.size - m + 1
+
+
+def test_every_band_layout_gives_the_same_join(gpu_dtwj, golden, synth, oracle):
+    # the autotuner may pick any layout: each must reproduce the result
+    x = synth.random_walk(3500, 6)
+    ref = oracle.join(x, 100, 52)
+    cases = [(c["series"], c["m"], c["w"], c["i"], c["j"], c["dist"]) for c in golden[:2]]
+    cases.append((x, 100, 52, ref.i, ref.j, ref.dist))
+    for xs, m, w, i, j, d in cases:
+        shapes = gpu_dtwj.band_shapes(min(w, m - 1))
+        assert len(shapes) >= 2
+        with gpu_dtwj.Context() as ctx:
+            for C, G in shapes:
+                ctx.set_band(min(w, m - 1), C, G)
+                _check(ctx.join(xs, m, w), i, j, d, (m, w, C, G))
+
+
+def test_autotune_measures_and_applies(gpu_dtwj, tmp_path):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "dtwj.autotune", os.path.join(PKG_DIR, "autotune.py"))
+    at = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(at)
+    path = str(tmp_path / "tune.json")
+    with gpu_dtwj.Context() as ctx:
+        e = at.apply(ctx, 128, 6, path, pairs=512)
+    assert e["cells_per_s"] > 0 and e["C"] * e["G"] >= 13
+    assert all(t[2] > 0 for t in e["tried"])
