@@ -197,6 +197,14 @@ int dtwj_ctx_set_model(dtwj_ctx* ctx, dtwj_mlp* net);
 int dtwj_ctx_tiles(dtwj_ctx* ctx, const double* x, int64_t n, int32_t m, int32_t w,
                    int64_t* count, int32_t* desc, float* features, double* min_dist);
 
+/* Sharding one join over several GPUs (no counterpart in the reference): a
+ * context with shard (rank, world) joins only the diagonal-sweep tiles t with
+ * t % world == rank, its ED-profile seeds included.  The tiles are disjoint
+ * sets of pairs covering every pair, so the lexicographic minimum of
+ * (dist, i, j) over the world's results is the single-context result.  The
+ * counters of each result cover its shard.  (0, 1) restores the whole join. */
+int dtwj_ctx_set_shard(dtwj_ctx* ctx, int32_t rank, int32_t world);
+
 /* ---- Autotuning of the DTW band layout (no counterpart in the reference;
  * the reference fixes its layout at compile time with REGISTER_NUM) ----
  * The banded DTW runs a group of G lanes per pair with C band cells per lane

@@ -74,6 +74,7 @@ EXPORTS = (
     "dtwj_band_shapes",
     "dtwj_time_band",
     "dtwj_ctx_set_band",
+    "dtwj_ctx_set_shard",
 )
 
 MLP_IN = 64
@@ -193,6 +194,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dtwj_band_shapes.argtypes = [i32, P(i32), P(i32), i32]
     lib.dtwj_time_band.argtypes = [ctypes.c_int, i32, i32, i32, i32, i32, P(d)]
     lib.dtwj_ctx_set_band.argtypes = [vp, i32, i32, i32]
+    lib.dtwj_ctx_set_shard.argtypes = [vp, i32, i32]
     lib.dtwj_ctx_tiles.argtypes = [vp, P(d), i64, i32, i32, P(i64), P(i32), f32p, P(d)]
     _lib = lib
     return lib
@@ -277,6 +279,12 @@ class Context:
         if rc != OK:
             raise DtwjError(rc, "dtwj_ctx_join")
         return JoinResult._from(r)
+
+    def set_shard(self, rank: int, world: int):
+        """Join only the tiles t with t % world == rank (dtwj_ctx_set_shard)."""
+        rc = load().dtwj_ctx_set_shard(self._h, rank, world)
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_set_shard")
 
     def set_band(self, w: int, C: int = 0, G: int = 0):
         """Joins with band w use the DTW layout (C cells per lane, G lanes per
@@ -476,3 +484,48 @@ def time_band(m: int, w: int, C: int, G: int, pairs: int = 2048, device: int = 0
     if rc != OK:
         raise DtwjError(rc, "dtwj_time_band")
     return v.value
+
+
+_COUNTERS = ("pairs", "pruned_fast", "pruned_kim", "pruned_masked", "pruned_keogh", "dtw_calls",
+             "dtw_abandoned", "dtw_cells", "candidates")
+
+
+def merge_results(results) -> JoinResult:
+    """One join's result from its shards' results: the lexicographic minimum
+    of (dist, i, j) (a shard without a pair, i = -1, never wins), counters
+    summed, times the maximum, seed_bsf the minimum."""
+    rs = list(results)
+    have = [r for r in rs if r.i >= 0]
+    best = min(have, key=lambda r: (r.dist, r.i, r.j)) if have else rs[0]
+    d = dict(best.__dict__)
+    for k in _COUNTERS:
+        d[k] = sum(getattr(r, k) for r in rs)
+    d["seconds_join"] = max(r.seconds_join for r in rs)
+    d["seconds_total"] = max(r.seconds_total for r in rs)
+    d["seed_bsf"] = min(r.seed_bsf for r in rs)
+    d["phase_seconds"] = [max(v) for v in zip(*(r.phase_seconds for r in rs))]
+    d["phase_launches"] = [sum(v) for v in zip(*(r.phase_launches for r in rs))]
+    return JoinResult(**d)
+
+
+def join_sharded(x, m: int, w: int, flags: int = 0, device: int | None = None, group=None,
+                 result_fn=None) -> JoinResult:
+    """One join spread over the ranks of a torch.distributed process group:
+    rank r sweeps the tiles t with t % world == r on its device (default: the
+    current CUDA device) and the ranks exchange only their results (one
+    all_gather of a few numbers).  result_fn(rank, world) replaces the device
+    join (tests of the exchange without a GPU)."""
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    if result_fn is not None:
+        mine = result_fn(rank, world)
+    else:
+        if device is None:
+            import torch
+            device = torch.cuda.current_device()
+        with Context(device) as ctx:
+            ctx.set_shard(rank, world)
+            mine = ctx.join(x, m, w, flags)
+    gathered = [None] * world
+    dist.all_gather_object(gathered, mine.__dict__, group=group)
+    return merge_results(JoinResult(**g) for g in gathered)

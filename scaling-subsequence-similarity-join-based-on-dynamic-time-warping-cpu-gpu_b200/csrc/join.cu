@@ -61,6 +61,7 @@ struct dtwj_ctx {
   std::vector<Tile> tiles_run;             // the tiles in the order of the current call
   dtwj_mlp* model = nullptr;               // scores tiles for DTWJ_F_LEARNED (not owned)
   std::vector<std::pair<int, BandShape>> band_override;  // band w -> DTW layout (autotuner)
+  int shard_rank = 0, shard_world = 1;  // this context sweeps tiles t with t % world == rank
   std::vector<cudaEvent_t> pool;  // events for per-phase device times
   // the sweep's launches captured as a CUDA graph, replayed while every
   // launch argument is unchanged (same buffers, tiles, band, flags)
@@ -347,12 +348,20 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   if (rc) return rc;
 
   build_lb_tiles(ctx, n, m, sbeg, nseries);
-  const int nlb = (int)ctx->lbtiles_host.size();
+  std::vector<Tile>& th = ctx->tiles_run;
+  th = ctx->lbtiles_host;
+  if (ctx->shard_world > 1 && !tq) {
+    // one shard of the tiles (round robin): the profile, the seeds and the
+    // sweep only see these; the shards' results combine by their minimum
+    size_t k = 0;
+    for (size_t t = 0; t < th.size(); ++t)
+      if ((int)(t % (size_t)ctx->shard_world) == ctx->shard_rank) th[k++] = th[t];
+    th.resize(k);
+  }
+  const int nlb = (int)th.size();
   // best-so-far slots: one per series, or one per tile for the tile minima
   const int nslots = tile_mode ? (nlb > 0 ? nlb : 1) : nseries;
   S.nseries = nslots;
-  std::vector<Tile>& th = ctx->tiles_run;
-  th = ctx->lbtiles_host;
   if (tile_mode)
     for (int t = 0; t < nlb; ++t) th[t].series = t;
   Tile* lbtiles;
@@ -440,8 +449,9 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
         if (na != nb) return nb;
         return !na && sc[a] < sc[b];
       });
+      const std::vector<Tile> plain = th;
       for (int t = 0; t < nlb; ++t) {
-        th[t] = ctx->lbtiles_host[ord[t]];
+        th[t] = plain[ord[t]];
         th[t].order = t;
       }
       CUDA_OK(cudaMemcpyAsync(lbtiles, th.data(), (size_t)nlb * sizeof(Tile),
@@ -816,6 +826,13 @@ int dtwj_time_band(int device, int32_t m, int32_t w, int32_t C, int32_t G, int32
   } while (0);
   dtwj_ctx_destroy(ctx);
   return rc;
+}
+
+int dtwj_ctx_set_shard(dtwj_ctx* ctx, int32_t rank, int32_t world) {
+  if (!ctx || world < 1 || rank < 0 || rank >= world) return DTWJ_ERR_ARG;
+  ctx->shard_rank = rank;
+  ctx->shard_world = world;
+  return DTWJ_OK;
 }
 
 int dtwj_ctx_set_model(dtwj_ctx* ctx, dtwj_mlp* net) {

@@ -225,3 +225,19 @@ def test_autotune_measures_and_applies(gpu_dtwj, tmp_path):
         e = at.apply(ctx, 128, 6, path, pairs=512)
     assert e["cells_per_s"] > 0 and e["C"] * e["G"] >= 13
     assert all(t[2] > 0 for t in e["tried"])
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_join_equals_the_whole(gpu_dtwj, golden, world):
+    # the shards of one join (run one after the other on this GPU) merge into
+    # the whole join's result; every pair is counted by exactly one shard
+    for c in [g for g in golden if g["name"] in ("rw20k", "rw6k_m128_w6")]:
+        whole = gpu_dtwj.join(c["series"], c["m"], c["w"])
+        parts = []
+        with gpu_dtwj.Context() as ctx:
+            for r in range(world):
+                ctx.set_shard(r, world)
+                parts.append(ctx.join(c["series"], c["m"], c["w"]))
+        merged = gpu_dtwj.merge_results(parts)
+        _check(merged, c["i"], c["j"], c["dist"], (c["name"], world))
+        assert merged.pairs == whole.pairs
