@@ -283,6 +283,21 @@ def run_ours(args):
                 for k, p in enumerate(dtwj.PHASES)}
     dominant = max(phases, key=phases.get)
 
+    # the same join in the learned tile order (the committed network), for
+    # the plain-vs-learned comparison the metric names; top-1 must not change
+    learned = None
+    model_path = os.path.join(os.path.dirname(dtwj.LIB_PATH), "..", "tile_mlp_rw_m256.bin")
+    if os.path.exists(model_path) and not args.no_learned:
+        net = dtwj.MLP.load_file(os.path.abspath(model_path), device=local)
+        ctx.set_model(net)
+        rl = [ctx.join_device(dptr, n, m, w, flags | dtwj.F_LEARNED) for _ in range(2)][-1]
+        learned = {"join_seconds": rl.seconds_join, "plain_join_seconds": r0.seconds_join,
+                   "dtw_calls": rl.dtw_calls, "plain_dtw_calls": r0.dtw_calls,
+                   "identical_top1": (rl.i, rl.j, rl.dist) == (r0.i, r0.j, r0.dist)
+                   if world == 1 else None,
+                   "model": "tile_mlp_rw_m256.bin (trained on m=256 random walks)"}
+        ctx.set_model(None)
+
     # e2e through the host-pointer API (pinned host buffer)
     fn = dtwj.load().dtwj_ctx_join
     R = dtwj._Result
@@ -297,25 +312,39 @@ def run_ours(args):
     e2e_wall = _max_over_ranks(time.perf_counter() - t1, dist, local)
 
     hbm_peak, peak_kind, sm_max = _peaks()
-    # algorithmic bytes of the diagonal sweep: every tile streams its row and
-    # column slices of the per-index arrays once (8 FP64 row/column arrays for
-    # the fast bound + mask/series/envelope slices of the masked bound).
-    tiles_rows = 0
-    for L0 in range(m, s, 128):
+    # Algorithmic DRAM bytes of the three sweep kernels over one join (the
+    # data each must move at least once; averaged per launch below):
+    #   k_lb    reads the six per-index FP64 operands of its rows and columns
+    #           ((2 rows + 896 lags) x 48 B per tile) and writes the survivor
+    #           bits (896 lags x 126 words x 4 B per tile)
+    #   k_runs  reads those bits and writes one 16-byte LB_Keogh candidate per
+    #           pair that passes the masked and endpoint bounds
+    #   k_keogh reads the candidates and writes an 8-byte DTW entry per survivor
+    ntiles, rows_sum = 0, 0
+    for L0 in range(m, s, 896):
         rows = s - L0
-        tiles_rows += rows + (rows + 4095) // 4096 * 128
-    bytes_per_index = 8 * 8 + (4 + 8 + 8) * 2
-    diag_bytes = tiles_rows * 2 * bytes_per_index
-    diag_launches = max(1, launches["diag"])
-    per_launch_s = phases["diag"] / diag_launches
-    achieved_gbs = diag_bytes / max(phases["diag"], 1e-12) / 1e9
-    fp64_flops = pairs_total * 32.0  # 8 FP64 accumulators x 2 DFMA per pair
-    fp64_peak = 148 * 64 * 2 * sm_max * 1e6 / 1e12
+        ntiles += (rows + 4031) // 4032
+        rows_sum += rows
+    bits_bytes = ntiles * 896 * 126 * 4
+    kq_entries = r0.pruned_keogh + r0.dtw_calls  # pairs that reached LB_Keogh (seeds aside)
+    alg = {
+        "diag": ("k_lb", (2 * rows_sum + ntiles * 896) * 48 + bits_bytes),
+        "runs": ("k_runs", bits_bytes + 16 * kq_entries),
+        "keogh": ("k_keogh", 16 * kq_entries + 8 * r0.dtw_calls),
+    }
+    sweep_phases = [p for p in ("runs", "keogh", "diag") if phases.get(p, 0) > 0]
+    roof_phase = max(sweep_phases, key=lambda p: phases[p]) if sweep_phases else "diag"
+    kname, alg_bytes = alg[roof_phase]
+    nl = max(1, launches[roof_phase])
+    per_launch_s = phases[roof_phase] / nl
+    achieved_gbs = alg_bytes / max(phases[roof_phase], 1e-12) / 1e9
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "diag_sweep_traffic.json")
-    if os.path.exists(tfile):
+    tfile = os.path.join(ROOT, "profiles", "ncu_traffic_rw1m_motif.json")
+    if os.path.exists(tfile) and args.workload == "rw1m_motif":
         with open(tfile) as f:
-            traffic = json.load(f).get("bytes_per_launch_scaled")
+            traffic = json.load(f).get("bytes_per_launch", {}).get(kname)
+    fp64_flops = pairs_total * 12.0  # k_lb: 2 recurrences x 2 DFMA + 2 DFMA tests per pair
+    fp64_peak = 148 * 64 * 2 * sm_max * 1e6 / 1e12
     cells_per_s = r0.dtw_cells / max(phases.get("pairs", 1e-12) + phases.get("seeds", 0), 1e-12)
 
     cpu = None
@@ -350,16 +379,20 @@ def run_ours(args):
                    "dtw_abandoned": r0.dtw_abandoned},
         "dtw_cells_per_s": cells_per_s,
         "phase_seconds": phases,
-        "roofline": {"bound": "hbm", "kernel": "diag sweep (k_lb)", "achieved": achieved_gbs,
-                     "peak": hbm_peak, "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
-                     "traffic": traffic, "peak_kind": peak_kind,
-                     "per_launch_ms": 1000 * per_launch_s},
-        "issue_roofline": {"pipe": "fp64", "kernel": "diag sweep (k_lb)",
+        "roofline": {"bound": "hbm", "kernel": kname, "phase": roof_phase,
+                     "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg_bytes / nl,
+                     "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                     "per_launch_ms": 1000 * per_launch_s,
+                     "note": "issue-bound, not HBM-bound: see profiles/"},
+        "issue_roofline": {"pipe": "fp64", "kernel": "k_lb",
                            "achieved": fp64_flops / max(phases["diag"], 1e-12) / 1e12,
                            "peak": fp64_peak, "unit": "TFLOP/s",
                            "frac": fp64_flops / max(phases["diag"], 1e-12) / 1e12 / fp64_peak,
                            "peak_kind": "nominal 148 SM x 64 DFMA/clk x max clock"},
         "dominant_phase": dominant,
+        "learned_order": learned,
         "cpu_baseline": cpu,
         "e2e": {"value": pairs_total * args.steps / e2e_wall, "unit": UNIT,
                 "h2d_bytes_per_step": int(x.nbytes), "d2h_bytes_per_step": 360},
@@ -385,6 +418,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=16384)
     ap.add_argument("--ref-sample", type=int, default=8192)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
