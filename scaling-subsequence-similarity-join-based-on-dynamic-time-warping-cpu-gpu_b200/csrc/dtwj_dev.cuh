@@ -49,7 +49,6 @@ struct Tile {
   int32_t send;    // end of the series' windows (global window index)
   int32_t series;  // series of the batch (0 for a single join)
 };
-constexpr int kTileLags = 128;
 // Diagonal-sweep tiles: 128 threads x kLbPerThread lags x kLbRows rows, one
 // survivor bit per pair, kLbWords 32-row words per lag.
 constexpr int kLbThreads = 128;
@@ -136,7 +135,7 @@ struct DevSearch {
   unsigned int* queue_count;
   unsigned int* queue_next;
   unsigned int queue_cap;
-  int4* kq;                     // LB_Keogh candidates: (i, j, endpoint bound bits, 0)
+  int4* kq;                     // LB_Keogh candidates: (i, j, endpoint bound bits, series)
   unsigned int* kq_count;
   unsigned int* kq_next;
   unsigned int kq_cap;

@@ -30,7 +30,6 @@ using namespace dtwj;
 
 namespace {
 
-constexpr int kTileRows = 4096;
 constexpr unsigned int kCandCap = 1u << 20;
 constexpr unsigned int kQueueCapMax = 1u << 26;
 constexpr int kLbChunkTiles = 1024;

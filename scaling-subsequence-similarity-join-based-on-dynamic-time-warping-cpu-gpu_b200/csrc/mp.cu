@@ -24,8 +24,6 @@
 namespace dtwj {
 namespace {
 
-constexpr int kMpRowsMax = 4096;
-
 // Row minima of ED^2 over the upper triangle (partners j >= i + m).  Tile and
 // staging as in the diagonal sweep (lb.cu): 128 threads x kLbPerThread lags
 // x kLbRows rows, column operands (df[j-1], dg[j-1], 1/sig_j and the flat

@@ -56,7 +56,8 @@ template <int G>
 __device__ __forceinline__ unsigned int group_mask() {
   if (G == 32) return 0xffffffffu;
   const unsigned int lane = threadIdx.x & 31;
-  return ((1u << G) - 1u) << (lane & ~(unsigned)(G - 1));
+  constexpr unsigned int bits = G < 32 ? (1u << (G % 32)) - 1u : 0xffffffffu;
+  return bits << (lane & ~(unsigned)(G - 1));
 }
 
 template <int G, typename V>
