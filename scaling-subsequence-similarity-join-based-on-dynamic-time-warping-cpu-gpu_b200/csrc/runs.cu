@@ -206,7 +206,7 @@ __device__ int cut_runs(const unsigned int* w, int* pos, int2* list, int cap) {
 
 constexpr int kRunList = 32;
 
-__global__ void __launch_bounds__(kRunWarps * 32) k_runs(DevSeries S, DevSearch Q,
+__global__ void __launch_bounds__(kRunWarps * 32, 8) k_runs(DevSeries S, DevSearch Q,
                                                          const Tile* tiles,
                                                          const unsigned int* bits,
                                                          unsigned int total_items, bool masked,
