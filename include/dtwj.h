@@ -219,6 +219,29 @@ int dtwj_time_band(int device, int32_t m, int32_t w, int32_t C, int32_t G, int32
                    double* cells_per_s);
 int dtwj_ctx_set_band(dtwj_ctx* ctx, int32_t w, int32_t C, int32_t G);
 
+/* Series files in the formats of the reference's loaders
+ * (CPU_version1/loadfile.cpp:14-142, GPU_version1/src/loadfile.cu:13-148):
+ *   DTWJ_LOAD_VALUES        every whitespace-separated number (loadfile)
+ *   DTWJ_LOAD_EVERY         every param-th of them, from the first (loadfile_apart)
+ *   DTWJ_LOAD_FIRST_COLUMN  the first number of every non-empty line of path,
+ *                           then of path2 if it is not NULL (loadfile_2)
+ *   DTWJ_LOAD_ROWS          the lines as a matrix flattened row by row, each row
+ *                           cut to the first row's width (loadfile_); a shorter
+ *                           row returns DTWJ_ERR_IO (the reference reads past it)
+ *   DTWJ_LOAD_BINARY        raw little-endian float64
+ * A token that is not a number ends the read (of the file, or of its line for
+ * the line formats), as the reference's stream extraction does.  *n = the
+ * series length; up to cap values go to out (out may be NULL with cap 0, to
+ * size the buffer).  DTWJ_ERR_IO if a file cannot be read (the reference
+ * exits instead). */
+#define DTWJ_LOAD_VALUES 0
+#define DTWJ_LOAD_EVERY 1
+#define DTWJ_LOAD_FIRST_COLUMN 2
+#define DTWJ_LOAD_ROWS 3
+#define DTWJ_LOAD_BINARY 4
+int dtwj_load(const char* path, const char* path2, int32_t format, int32_t param, double* out,
+              int64_t cap, int64_t* n);
+
 /* Band from a ratio: ceil(ratio*m) (rounding=0) or the reference's
  * max(round(ratio*m), 1) (rounding=1, GPU_version1/src/AAAA.cu:34). */
 int32_t dtwj_band(int32_t m, double ratio, int32_t rounding);

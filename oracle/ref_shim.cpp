@@ -11,6 +11,8 @@
 //   ref_mvmean    -> mvmean                 CPU_version1/allmatrixop/movmean.cpp:9
 //   ref_lemire    -> lower_upper_lemire     CPU_version1/allmatrixop/lower_upper_lemire.cpp:7
 //   ref_mpx       -> mpx_v2                 CPU_version1/mpx_v2.cpp:13
+//   ref_load      -> loadfile / loadfile_apart / loadfile_2 / loadfile_
+//                                           CPU_version1/loadfile.cpp:14,35,63,114
 #include "alldef/matrix.h"
 #include "alldef/allstruct.h"
 #include "allunder/underdtw.h"
@@ -25,6 +27,10 @@
 #include <chrono>
 
 RETURN_MPX mpx_v2(const vector<DOUBLE>& timeSeries, int minlag, int subseqlen);
+vector<DOUBLE> loadfile(string filename);
+vector<DOUBLE> loadfile_apart(string filename, int apart);
+vector<DOUBLE> loadfile_2(string filename1, string filename2);
+vector<DOUBLE> loadfile_(string filename);
 void DTWMotifDiscoveryGUI(const vector<DOUBLE>& TS, int subseqlen, int maxwarp,
                           const char* output_time_file_path);
 
@@ -139,6 +145,21 @@ int ref_join(const double* x, long n, int m, int w, const char* timefile,
     *dist_full = std::sqrt(MON_dtw(q, t, cb, m, w, 1e300));
   }
   return 0;
+}
+
+// The reference's loaders: format 0 loadfile, 1 loadfile_apart(param),
+// 2 loadfile_2(path, path2), 3 loadfile_.  Writes up to cap values, returns
+// how many the loader produced.  (The reference exits on a file it cannot
+// open: call it with readable files only.)
+long ref_load(const char* path, const char* path2, int format, int param, double* out,
+              long cap) {
+  vector<DOUBLE> v;
+  if (format == 0) v = loadfile(path);
+  else if (format == 1) v = loadfile_apart(path, param);
+  else if (format == 2) v = loadfile_2(path, path2);
+  else v = loadfile_(path);
+  for (long k = 0; k < (long)v.size() && k < cap; ++k) out[k] = (double)v[(size_t)k];
+  return (long)v.size();
 }
 
 }  // extern "C"

@@ -75,7 +75,10 @@ EXPORTS = (
     "dtwj_time_band",
     "dtwj_ctx_set_band",
     "dtwj_ctx_set_shard",
+    "dtwj_load",
 )
+
+LOAD_FORMATS = {"values": 0, "every": 1, "first-column": 2, "rows": 3, "binary": 4}
 
 MLP_IN = 64
 MLP_HIDDEN = 128
@@ -195,6 +198,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dtwj_time_band.argtypes = [ctypes.c_int, i32, i32, i32, i32, i32, P(d)]
     lib.dtwj_ctx_set_band.argtypes = [vp, i32, i32, i32]
     lib.dtwj_ctx_set_shard.argtypes = [vp, i32, i32]
+    lib.dtwj_load.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, P(d), i64, P(i64)]
     lib.dtwj_ctx_tiles.argtypes = [vp, P(d), i64, i32, i32, P(i64), P(i32), f32p, P(d)]
     _lib = lib
     return lib
@@ -529,3 +533,22 @@ def join_sharded(x, m: int, w: int, flags: int = 0, device: int | None = None, g
     gathered = [None] * world
     dist.all_gather_object(gathered, mine.__dict__, group=group)
     return merge_results(JoinResult(**g) for g in gathered)
+
+
+def load_series(path: str, fmt: str = "values", every: int = 1, path2: str | None = None):
+    """A series file in one of the reference's formats (dtwj_load): "values"
+    (loadfile), "every" (loadfile_apart, every `every`-th value), "first-column"
+    (loadfile_2: first number of each line of path, then path2), "rows"
+    (loadfile_: lines flattened row by row) or "binary" (raw float64)."""
+    lib = load()
+    n = ctypes.c_int64()
+    p1, p2 = path.encode(), (path2.encode() if path2 else None)
+    f = LOAD_FORMATS[fmt]
+    rc = lib.dtwj_load(p1, p2, f, every, None, 0, ctypes.byref(n))
+    if rc != OK:
+        raise DtwjError(rc, "dtwj_load")
+    out = np.empty(n.value, dtype=np.float64)
+    rc = lib.dtwj_load(p1, p2, f, every, _dptr(out), out.size, ctypes.byref(n))
+    if rc != OK:
+        raise DtwjError(rc, "dtwj_load")
+    return out

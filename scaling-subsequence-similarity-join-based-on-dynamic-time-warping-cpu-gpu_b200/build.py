@@ -24,7 +24,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
 CU_SOURCES = ["prep.cu", "mp.cu", "lb.cu", "runs.cu", "pairs.cu", "join.cu", "noalloc.cu", "mlp.cu",
-              "features.cu"]
+              "features.cu", "load.cpp"]
 
 
 def _nvcc() -> str:
@@ -64,7 +64,7 @@ def build(verbose: bool = False) -> str:
     objs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if _newer([s] + heads, o):
             jobs.append([nvcc] + ARCH + NVCC_FLAGS + ["-c", s, "-o", o])

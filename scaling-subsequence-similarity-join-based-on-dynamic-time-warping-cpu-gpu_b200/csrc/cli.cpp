@@ -13,7 +13,15 @@
 //   --band-rounding=ceil|round  w = ceil(ratio*m) (default) or the reference
 //                               executables' max(round(ratio*m), 1)
 //   --band=W                    explicit band, overrides the ratio
-//   --binary                    data file is raw little-endian float64
+//   --format=values|every|first-column|rows|binary
+//                               how the data file is read (dtwj_load): every
+//                               number (default, loadfile), every N-th
+//                               (loadfile_apart), the first number of each line
+//                               (loadfile_2, with --data2 as its second file),
+//                               a matrix row by row (loadfile_), raw float64
+//   --every=N                   N for --format=every
+//   --data2=PATH                second file for --format=first-column
+//   --binary                    same as --format=binary
 //   --json=PATH                 also write the full result as JSON
 //   --no-masked, --no-seed      disable the masked bound / ED seeding
 //   --verbose                   phase timings on stderr
@@ -23,33 +31,15 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <fstream>
 #include <string>
 #include <vector>
-
-static bool load_ascii(const char* path, std::vector<double>* out) {
-  std::ifstream f(path);
-  if (!f.is_open()) return false;
-  double v;
-  while (f >> v) out->push_back(v);
-  return true;
-}
-
-static bool load_binary(const char* path, std::vector<double>* out) {
-  FILE* f = fopen(path, "rb");
-  if (!f) return false;
-  double buf[8192];
-  size_t k;
-  while ((k = fread(buf, sizeof(double), 8192, f)) > 0) out->insert(out->end(), buf, buf + k);
-  fclose(f);
-  return true;
-}
 
 int main(int argc, char** argv) {
   if (argc < 5) {
     fprintf(stderr,
             "usage: %s <data_path> <time_out_path> <m> <ratio> [--band-rounding=ceil|round]"
-            " [--band=W] [--binary] [--json=PATH] [--no-masked] [--no-seed] [--verbose]\n",
+            " [--band=W] [--format=values|every|first-column|rows|binary] [--every=N]"
+            " [--data2=PATH] [--binary] [--json=PATH] [--no-masked] [--no-seed] [--verbose]\n",
             argv[0]);
     return 2;
   }
@@ -57,8 +47,8 @@ int main(int argc, char** argv) {
   const char* time_out = argv[2];
   const int m = atoi(argv[3]);
   const double ratio = atof(argv[4]);
-  int rounding = 0, band = -1;
-  bool binary = false;
+  int rounding = 0, band = -1, format = DTWJ_LOAD_VALUES, every = 1;
+  std::string data2;
   std::string json;
   uint32_t flags = 0;
   for (int k = 5; k < argc; ++k) {
@@ -66,7 +56,13 @@ int main(int argc, char** argv) {
     if (!strcmp(a, "--band-rounding=round")) rounding = 1;
     else if (!strcmp(a, "--band-rounding=ceil")) rounding = 0;
     else if (!strncmp(a, "--band=", 7)) band = atoi(a + 7);
-    else if (!strcmp(a, "--binary")) binary = true;
+    else if (!strcmp(a, "--binary") || !strcmp(a, "--format=binary")) format = DTWJ_LOAD_BINARY;
+    else if (!strcmp(a, "--format=values")) format = DTWJ_LOAD_VALUES;
+    else if (!strcmp(a, "--format=every")) format = DTWJ_LOAD_EVERY;
+    else if (!strcmp(a, "--format=first-column")) format = DTWJ_LOAD_FIRST_COLUMN;
+    else if (!strcmp(a, "--format=rows")) format = DTWJ_LOAD_ROWS;
+    else if (!strncmp(a, "--every=", 8)) every = atoi(a + 8);
+    else if (!strncmp(a, "--data2=", 8)) data2 = a + 8;
     else if (!strncmp(a, "--json=", 7)) json = a + 7;
     else if (!strcmp(a, "--no-masked")) flags |= DTWJ_F_NO_MASKED;
     else if (!strcmp(a, "--no-seed")) flags |= DTWJ_F_NO_SEED;
@@ -77,10 +73,21 @@ int main(int argc, char** argv) {
     }
   }
   std::vector<double> x;
-  const bool ok = binary ? load_binary(data, &x) : load_ascii(data, &x);
-  if (!ok) {
+  int64_t n = 0;
+  const char* d2 = data2.empty() ? nullptr : data2.c_str();
+  int lrc = dtwj_load(data, d2, format, every, nullptr, 0, &n);
+  if (lrc == DTWJ_OK) {
+    x.resize((size_t)n);
+    lrc = dtwj_load(data, d2, format, every, x.data(), n, &n);
+  }
+  if (lrc == DTWJ_ERR_IO) {
+    // as the reference: report and exit with 0 (GPU_version1/src/loadfile.cu:17-21)
     fprintf(stderr, "Error opening file: %s\n", data);
     return 0;
+  }
+  if (lrc != DTWJ_OK) {
+    fprintf(stderr, "dtwj: %s\n", dtwj_strerror(lrc));
+    return 2;
   }
   const int w = band >= 0 ? band : dtwj_band(m, ratio, rounding);
   printf("buffer_length: %d, maxwarp: %d\n", m, w);

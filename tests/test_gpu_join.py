@@ -241,3 +241,21 @@ def test_sharded_join_equals_the_whole(gpu_dtwj, golden, world):
         merged = gpu_dtwj.merge_results(parts)
         _check(merged, c["i"], c["j"], c["dist"], (c["name"], world))
         assert merged.pairs == whole.pairs
+
+
+def test_cli_reads_the_reference_file_formats(tmp_path, golden):
+    # the series split into the first column of two files (loadfile_2) and
+    # into a 4-column matrix (loadfile_) gives the same join as one column
+    c = [g for g in golden if g["name"] == "rw20k"][0]
+    x = np.asarray(c["series"])
+    half = x.size // 2
+    fa, fb, fm = tmp_path / "a.txt", tmp_path / "b.txt", tmp_path / "m.txt"
+    np.savetxt(fa, np.stack([x[:half], np.arange(half)], 1), fmt="%.17g")
+    np.savetxt(fb, x[half:], fmt="%.17g")
+    np.savetxt(fm, x.reshape(-1, 4), fmt="%.17g")
+    cli = os.path.join(PKG_DIR, "bin", "dtwj")
+    tf = tmp_path / "time.txt"
+    for extra, data in ((["--format=first-column", "--data2=%s" % fb], fa), (["--format=rows"], fm)):
+        out = subprocess.run([cli, str(data), str(tf), "256", "0.01"] + extra, capture_output=True,
+                             text=True, check=True).stdout
+        assert "first min is %d sec min is %d" % (c["i"] + 1, c["j"] + 1) in out, extra
