@@ -5,7 +5,30 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 namespace dtwj {
+
+// Runs a set-up step (a kernel attribute, which CUDA keeps per device) once
+// for each device a launch site is used on, also with several host threads.
+class OncePerDevice {
+ public:
+  template <class F>
+  void run(F f) {
+    int d = 0;
+    cudaGetDevice(&d);
+    const unsigned long long bit = 1ull << (d & 63);
+    std::lock_guard<std::mutex> lock(mu_);
+    if (!(done_ & bit)) {
+      f();
+      done_ |= bit;
+    }
+  }
+
+ private:
+  std::mutex mu_;
+  unsigned long long done_ = 0;
+};
 
 // Relative slack on squared distances for every pruning and abandoning test.
 // FP32 distances and the FP64 diagonal recurrences carry rounding error far

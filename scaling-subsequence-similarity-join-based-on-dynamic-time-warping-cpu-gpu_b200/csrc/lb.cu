@@ -235,11 +235,10 @@ void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int ti
                int tile_end, unsigned int* bits, bool enumerate_all, unsigned int* next,
                int num_sms, cudaStream_t st) {
   if (tile_end <= tile_begin) return;
-  static bool configured = false;
-  if (!configured) {
+  static OncePerDevice setup;
+  setup.run([] {
     cudaFuncSetAttribute(k_lb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LbShared));
-    configured = true;
-  }
+  });
   const int ntiles = tile_end - tile_begin;
   const int resident = 3 * num_sms;  // three CTAs per SM (launch bounds, 64.5 KB shared each)
   k_lb<<<ntiles < resident ? ntiles : resident, kLbThreads, sizeof(LbShared), st>>>(

@@ -328,11 +328,10 @@ void launch_mp(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long 
                cudaStream_t st, unsigned int* tile_best) {
   k_fill_u64<<<1024, 256, 0, st>>>(keys, S.s, ULLONG_MAX);
   if (ntiles <= 0) return;
-  static bool configured = false;
-  if (!configured) {
+  static OncePerDevice setup;
+  setup.run([] {
     cudaFuncSetAttribute(k_mp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MpShared));
-    configured = true;
-  }
+  });
   const int slab = 1 << 20;
   for (int b = 0; b < ntiles; b += slab) {
     const int cnt = ntiles - b < slab ? ntiles - b : slab;

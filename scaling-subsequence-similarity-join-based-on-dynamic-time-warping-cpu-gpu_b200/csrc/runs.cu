@@ -250,108 +250,108 @@ __global__ void __launch_bounds__(kRunWarps * 32, 8) k_runs(DevSeries S, DevSear
       __syncwarp();
       if (nr == 0) break;
       for (int ri = 0; ri < nr; ++ri) {
-    const int64_t i0 = (int64_t)T.i0 + rl[ri].x, j0 = i0 + L;
-    const int len = rl[ri].y;
-    if (!bounds) {
-      // no bounds: every pair of the run goes to the DTW stage
-      for (int p = lane; p < len; p += 32) {
-        const unsigned int slot = atomicAdd(Q.queue_count, 1u);
-        if (slot < Q.queue_cap) {
-          Q.queue[slot] = make_int2((int)(i0 + p), (int)(j0 + p));
-          if (Q.qser) Q.qser[slot] = T.series;
-        } else {
-          atomicOr(S.status, 2);
-        }
-      }
-      continue;
-    }
-    const unsigned int* bsf2 = Q.bsf2 + T.series;
-    float thr = prune_threshold_now(bsf2, S.m);
-    // ---- masked sums at the run's first pair (exact, FP64) ----
-    double F1 = 0, F2 = 0, F3 = 0, R1 = 0, R2 = 0, R3 = 0;
-    if (masked) {
-      for (int k = lo + lane; k <= hi; k += 32) {
-        const double ai = S.a[i0 + k], aj = S.a[j0 + k];
-        const double Mi = S.mask[i0 + k], Mj = S.mask[j0 + k];
-        F1 = fma(Mi, aj, F1);
-        F2 = fma(Mi * aj, aj, F2);
-        F3 = fma(Mi * S.E[i0 + k], aj, F3);
-        R1 = fma(Mj, ai, R1);
-        R2 = fma(Mj * ai, ai, R2);
-        R3 = fma(Mj * S.E[j0 + k], ai, R3);
-      }
-      F1 = warp_sum(F1);
-      F2 = warp_sum(F2);
-      F3 = warp_sum(F3);
-      R1 = warp_sum(R1);
-      R2 = warp_sum(R2);
-      R3 = warp_sum(R3);
-    }
-    for (int b = 0; b < len; b += 32) {
-      const int p = b + lane;
-      const bool valid = p < len;
-      const int64_t i = i0 + p, j = j0 + p;
-      double lbm = 0.0;
-      if (masked) {
-        // per-row increments: the window start (k = lo) of the previous row
-        // leaves, the window end (k = hi) of this row enters
-        double d1 = 0, d2 = 0, d3 = 0, e1 = 0, e2 = 0, e3 = 0;
-        if (valid && p > 0) {
-          const int64_t io = i - 1 + lo, in = i + hi, jo = j - 1 + lo, jn = j + hi;
-          const double Mio = S.mask[io], Min = S.mask[in], Mjo = S.mask[jo], Mjn = S.mask[jn];
-          const double ajo = S.a[jo], ajn = S.a[jn], aio = S.a[io], ain = S.a[in];
-          d1 = Min * ajn - Mio * ajo;
-          d2 = Min * ajn * ajn - Mio * ajo * ajo;
-          d3 = Min * S.E[in] * ajn - Mio * S.E[io] * ajo;
-          e1 = Mjn * ain - Mjo * aio;
-          e2 = Mjn * ain * ain - Mjo * aio * aio;
-          e3 = Mjn * S.E[jn] * ain - Mjo * S.E[jo] * aio;
-        }
-        const double f1 = F1 + warp_iscan(d1, lane), f2 = F2 + warp_iscan(d2, lane);
-        const double f3 = F3 + warp_iscan(d3, lane), r1 = R1 + warp_iscan(e1, lane);
-        const double r2 = R2 + warp_iscan(e2, lane), r3 = R3 + warp_iscan(e3, lane);
-        if (valid) lbm = fmax(masked_lb(S, i, j, f1, f2, f3), masked_lb(S, j, i, r1, r2, r3));
-        F1 = __shfl_sync(0xffffffffu, f1, 31);
-        F2 = __shfl_sync(0xffffffffu, f2, 31);
-        F3 = __shfl_sync(0xffffffffu, f3, 31);
-        R1 = __shfl_sync(0xffffffffu, r1, 31);
-        R2 = __shfl_sync(0xffffffffu, r2, 31);
-        R3 = __shfl_sync(0xffffffffu, r3, 31);
-      }
-      bool alive = valid;
-      if (alive && masked && lbm * lbm > (double)thr) {
-        alive = false;
-        atomicAdd(&cnt[kPrunedMasked], 1ull);
-      }
-      float kim = 0.0f;
-      if (alive) {
-        const ZEnds zi = z_ends(S, i), zj = z_ends(S, j);
-        double dl, dr;
-        kim_bound<double>(zi, zj, m, &dl, &dr);
-        kim = (float)(dl + dr);
-        if (dl + dr + lbm * lbm > (double)thr) {
-          alive = false;
-          atomicAdd(&cnt[kPrunedKim], 1ull);
-        }
-      }
-      // ---- survivors go to the LB_Keogh queue, in run order ----
-      const unsigned int bits = __ballot_sync(0xffffffffu, alive);
-      if (bits) {
-        unsigned int base = 0;
-        if (lane == 0) base = atomicAdd(Q.kq_count, (unsigned int)__popc(bits));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (alive) {
-          const unsigned int slot = base + __popc(bits & ((1u << lane) - 1u));
-          if (slot < Q.kq_cap) {
-            Q.kq[slot] = make_int4((int)i, (int)j, __float_as_int(kim), T.series);
-          } else {
-            atomicOr(S.status, 2);
+        const int64_t i0 = (int64_t)T.i0 + rl[ri].x, j0 = i0 + L;
+        const int len = rl[ri].y;
+        if (!bounds) {
+          // no bounds: every pair of the run goes to the DTW stage
+          for (int p = lane; p < len; p += 32) {
+            const unsigned int slot = atomicAdd(Q.queue_count, 1u);
+            if (slot < Q.queue_cap) {
+              Q.queue[slot] = make_int2((int)(i0 + p), (int)(j0 + p));
+              if (Q.qser) Q.qser[slot] = T.series;
+            } else {
+              atomicOr(S.status, 2);
+            }
           }
+          continue;
         }
-      }
-      // a fresh best-so-far tightens the rest of the run
-      thr = fminf(thr, prune_threshold_now(bsf2, S.m));
-    }
+        const unsigned int* bsf2 = Q.bsf2 + T.series;
+        float thr = prune_threshold_now(bsf2, S.m);
+        // ---- masked sums at the run's first pair (exact, FP64) ----
+        double F1 = 0, F2 = 0, F3 = 0, R1 = 0, R2 = 0, R3 = 0;
+        if (masked) {
+          for (int k = lo + lane; k <= hi; k += 32) {
+            const double ai = S.a[i0 + k], aj = S.a[j0 + k];
+            const double Mi = S.mask[i0 + k], Mj = S.mask[j0 + k];
+            F1 = fma(Mi, aj, F1);
+            F2 = fma(Mi * aj, aj, F2);
+            F3 = fma(Mi * S.E[i0 + k], aj, F3);
+            R1 = fma(Mj, ai, R1);
+            R2 = fma(Mj * ai, ai, R2);
+            R3 = fma(Mj * S.E[j0 + k], ai, R3);
+          }
+          F1 = warp_sum(F1);
+          F2 = warp_sum(F2);
+          F3 = warp_sum(F3);
+          R1 = warp_sum(R1);
+          R2 = warp_sum(R2);
+          R3 = warp_sum(R3);
+        }
+        for (int b = 0; b < len; b += 32) {
+          const int p = b + lane;
+          const bool valid = p < len;
+          const int64_t i = i0 + p, j = j0 + p;
+          double lbm = 0.0;
+          if (masked) {
+            // per-row increments: the window start (k = lo) of the previous row
+            // leaves, the window end (k = hi) of this row enters
+            double d1 = 0, d2 = 0, d3 = 0, e1 = 0, e2 = 0, e3 = 0;
+            if (valid && p > 0) {
+              const int64_t io = i - 1 + lo, in = i + hi, jo = j - 1 + lo, jn = j + hi;
+              const double Mio = S.mask[io], Min = S.mask[in], Mjo = S.mask[jo], Mjn = S.mask[jn];
+              const double ajo = S.a[jo], ajn = S.a[jn], aio = S.a[io], ain = S.a[in];
+              d1 = Min * ajn - Mio * ajo;
+              d2 = Min * ajn * ajn - Mio * ajo * ajo;
+              d3 = Min * S.E[in] * ajn - Mio * S.E[io] * ajo;
+              e1 = Mjn * ain - Mjo * aio;
+              e2 = Mjn * ain * ain - Mjo * aio * aio;
+              e3 = Mjn * S.E[jn] * ain - Mjo * S.E[jo] * aio;
+            }
+            const double f1 = F1 + warp_iscan(d1, lane), f2 = F2 + warp_iscan(d2, lane);
+            const double f3 = F3 + warp_iscan(d3, lane), r1 = R1 + warp_iscan(e1, lane);
+            const double r2 = R2 + warp_iscan(e2, lane), r3 = R3 + warp_iscan(e3, lane);
+            if (valid) lbm = fmax(masked_lb(S, i, j, f1, f2, f3), masked_lb(S, j, i, r1, r2, r3));
+            F1 = __shfl_sync(0xffffffffu, f1, 31);
+            F2 = __shfl_sync(0xffffffffu, f2, 31);
+            F3 = __shfl_sync(0xffffffffu, f3, 31);
+            R1 = __shfl_sync(0xffffffffu, r1, 31);
+            R2 = __shfl_sync(0xffffffffu, r2, 31);
+            R3 = __shfl_sync(0xffffffffu, r3, 31);
+          }
+          bool alive = valid;
+          if (alive && masked && lbm * lbm > (double)thr) {
+            alive = false;
+            atomicAdd(&cnt[kPrunedMasked], 1ull);
+          }
+          float kim = 0.0f;
+          if (alive) {
+            const ZEnds zi = z_ends(S, i), zj = z_ends(S, j);
+            double dl, dr;
+            kim_bound<double>(zi, zj, m, &dl, &dr);
+            kim = (float)(dl + dr);
+            if (dl + dr + lbm * lbm > (double)thr) {
+              alive = false;
+              atomicAdd(&cnt[kPrunedKim], 1ull);
+            }
+          }
+          // ---- survivors go to the LB_Keogh queue, in run order ----
+          const unsigned int bits = __ballot_sync(0xffffffffu, alive);
+          if (bits) {
+            unsigned int base = 0;
+            if (lane == 0) base = atomicAdd(Q.kq_count, (unsigned int)__popc(bits));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (alive) {
+              const unsigned int slot = base + __popc(bits & ((1u << lane) - 1u));
+              if (slot < Q.kq_cap) {
+                Q.kq[slot] = make_int4((int)i, (int)j, __float_as_int(kim), T.series);
+              } else {
+                atomicOr(S.status, 2);
+              }
+            }
+          }
+          // a fresh best-so-far tightens the rest of the run
+          thr = fminf(thr, prune_threshold_now(bsf2, S.m));
+        }
       }
       __syncwarp();
     }
