@@ -381,6 +381,12 @@ def run_ours(args):
                    "keogh": r0.pruned_keogh, "dtw_calls": r0.dtw_calls,
                    "dtw_abandoned": r0.dtw_abandoned},
         "dtw_cells_per_s": cells_per_s,
+        # DTW stage against its issue roofline: 5 operations per band cell
+        # (subtract, square-add, three-input minimum, band mask) on 148 SMs x
+        # 128 lanes at the maximum SM clock
+        "dtw_roofline": {"achieved": cells_per_s, "peak": 148 * 128 * sm_max * 1e6 / 5.0,
+                         "unit": "cells/s",
+                         "frac": cells_per_s / (148 * 128 * sm_max * 1e6 / 5.0)},
         "phase_seconds": phases,
         "roofline": {"bound": "hbm", "kernel": kname, "phase": roof_phase,
                      "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
