@@ -114,6 +114,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def sweep_tiles(n: int, m: int):
+    """(tiles, summed rows of the lag groups) of the diagonal sweep of one
+    series: lag groups of 896 lags from m, each split into tiles of at most
+    4032 rows, as the library lays them out."""
+    s = n - m + 1
+    ntiles, rows_sum = 0, 0
+    for L0 in range(m, s, 896):
+        rows = s - L0
+        ntiles += (rows + 4031) // 4032
+        rows_sum += rows
+    return ntiles, rows_sum
+
+
 def _dist_init():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -323,11 +336,7 @@ def run_ours(args):
     #   k_runs  reads those bits and writes one 16-byte LB_Keogh candidate per
     #           pair that passes the masked and endpoint bounds
     #   k_keogh reads the candidates and writes an 8-byte DTW entry per survivor
-    ntiles, rows_sum = 0, 0
-    for L0 in range(m, s, 896):
-        rows = s - L0
-        ntiles += (rows + 4031) // 4032
-        rows_sum += rows
+    ntiles, rows_sum = sweep_tiles(n, m)
     bits_bytes = ntiles * 896 * 126 * 4
     kq_entries = r0.pruned_keogh + r0.dtw_calls  # pairs that reached LB_Keogh (seeds aside)
     alg = {
