@@ -6,6 +6,10 @@
 #
 #   oracle/build_ref.sh [REFERENCE_ROOT]
 #
+# REFERENCE_ROOT defaults to $DTWJ_REFERENCE_ROOT, else /root/reference (where
+# the reference tree is mounted on the machine that builds the fixtures).
+# Exit code 2: no reference sources there (nothing built).
+#
 # Produces
 #   oracle/_ref/libref.so   C ABI around the reference functions (ref_shim.cpp)
 #   oracle/_ref/ref_join    one reference join per process (ref_join_main.cpp)
@@ -15,7 +19,7 @@
 # `-include` supplies the <cstring> several reference files forget).
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}/CPU_version1"
+REF="${1:-${DTWJ_REFERENCE_ROOT:-/root/reference}}/CPU_version1"
 OUT="$HERE/_ref"
 OBJ="$OUT/obj"
 if [ ! -d "$REF" ]; then

@@ -96,48 +96,18 @@ void orc_envelope(const double* a, int64_t n, int r, double* lower, double* uppe
   free(ql);
 }
 
-/* Squared banded DTW, exact (no pruning).  Cells (r, c) with |r - c| <= w. */
-double orc_dtw2(const double* q, const double* t, int m, int w) {
+/* Squared banded DTW, exact (no pruning).  Cells (r, c) with |r - c| <= w.
+ * Row buffers hold cell (r, c) at index c + 1; only the band is touched per
+ * row (index c0 is reset to +inf as the left border, indices right of the
+ * band have never been written and stay +inf). */
+static double dtw2_rows(const double* q, const double* t, const double* cb, int m, int w,
+                        double bsf2, double* prev, double* cur) {
   if (w > m) w = m;
-  double* prev = (double*)malloc(sizeof(double) * (size_t)(m + 1));
-  double* cur = (double*)malloc(sizeof(double) * (size_t)(m + 1));
-  for (int c = 0; c <= m; ++c) prev[c] = ORC_INF;
-  for (int r = 0; r < m; ++r) {
-    int c0 = r - w > 0 ? r - w : 0, c1 = r + w < m - 1 ? r + w : m - 1;
-    for (int c = 0; c <= m; ++c) cur[c] = ORC_INF;
-    for (int c = c0; c <= c1; ++c) {
-      double best;
-      if (r == 0 && c == 0) best = 0.0;
-      else {
-        double up = prev[c + 1], left = cur[c], diag = prev[c];
-        best = up < left ? up : left;
-        best = best < diag ? best : diag;
-      }
-      cur[c + 1] = best + sq(q[r] - t[c]);
-    }
-    double* tmp = prev; prev = cur; cur = tmp;
-  }
-  double d = prev[m];
-  free(prev);
-  free(cur);
-  return d;
-}
-
-/* Early-abandoning squared DTW (the semantics of MON_dtw): returns the exact
- * squared DTW when it is <= bsf2, otherwise ORC_INF or a value > bsf2.  After
- * row r every path still has to cross rows/columns >= r + w + 1, whose cost
- * is bounded below by cb[r + w + 1] (cb is a suffix sum, zero past m). */
-double orc_dtw2_ea(const double* q, const double* t, const double* cb, int m, int w,
-                   double bsf2) {
-  if (w > m) w = m;
-  double* prev = (double*)malloc(sizeof(double) * (size_t)(m + 1));
-  double* cur = (double*)malloc(sizeof(double) * (size_t)(m + 1));
-  for (int c = 0; c <= m; ++c) prev[c] = ORC_INF;
-  double result = ORC_INF;
+  for (int c = 0; c <= m + 1; ++c) { prev[c] = ORC_INF; cur[c] = ORC_INF; }
   int r;
   for (r = 0; r < m; ++r) {
     int c0 = r - w > 0 ? r - w : 0, c1 = r + w < m - 1 ? r + w : m - 1;
-    for (int c = 0; c <= m; ++c) cur[c] = ORC_INF;
+    cur[c0] = ORC_INF;
     double rowmin = ORC_INF;
     for (int c = c0; c <= c1; ++c) {
       double best;
@@ -151,14 +121,32 @@ double orc_dtw2_ea(const double* q, const double* t, const double* cb, int m, in
       cur[c + 1] = v;
       if (v < rowmin) rowmin = v;
     }
-    double rest = (r + w + 1 < m) ? cb[r + w + 1] : 0.0;
-    if (rowmin + rest > bsf2) break;
+    if (cb) {
+      double rest = (r + w + 1 < m) ? cb[r + w + 1] : 0.0;
+      if (rowmin + rest > bsf2) return ORC_INF;
+    }
     double* tmp = prev; prev = cur; cur = tmp;
   }
-  if (r == m) result = prev[m];
-  free(prev);
-  free(cur);
-  return result;
+  return prev[m];
+}
+
+double orc_dtw2(const double* q, const double* t, int m, int w) {
+  double* buf = (double*)malloc(sizeof(double) * (size_t)(2 * m + 4));
+  double d = dtw2_rows(q, t, NULL, m, w, ORC_INF, buf, buf + m + 2);
+  free(buf);
+  return d;
+}
+
+/* Early-abandoning squared DTW (the semantics of MON_dtw): returns the exact
+ * squared DTW when it is <= bsf2, otherwise ORC_INF.  After row r every path
+ * still has to cross rows/columns >= r + w + 1, whose cost is bounded below
+ * by cb[r + w + 1] (cb is a suffix sum, zero past m; MON_DTW.cpp:48). */
+double orc_dtw2_ea(const double* q, const double* t, const double* cb, int m, int w,
+                   double bsf2) {
+  double* buf = (double*)malloc(sizeof(double) * (size_t)(2 * m + 4));
+  double d = dtw2_rows(q, t, cb, m, w, bsf2, buf, buf + m + 2);
+  free(buf);
+  return d;
 }
 
 /* ED matrix profile with exclusion zone m (mpx_v2, minlag = m): diagonal
@@ -170,7 +158,12 @@ void orc_mp(const double* a, int64_t n, int m, double* mp, int64_t* mpi) {
   double* sig = (double*)malloc(sizeof(double) * (size_t)s);
   orc_stats(a, n, m, mu, sig);
   double* corr_best = (double*)malloc(sizeof(double) * (size_t)s);
-  for (int64_t i = 0; i < s; ++i) { corr_best[i] = -ORC_INF; mpi[i] = -1; }
+  unsigned char* flat = (unsigned char*)malloc((size_t)s);
+  for (int64_t i = 0; i < s; ++i) {
+    corr_best[i] = -ORC_INF;
+    mpi[i] = -1;
+    flat[i] = (unsigned char)is_flat(mu[i], sig[i]);
+  }
 #pragma omp parallel
   {
     double* cb = (double*)malloc(sizeof(double) * (size_t)s);
@@ -192,7 +185,7 @@ void orc_mp(const double* a, int64_t n, int m, double* mp, int64_t* mpi) {
           double dgj = (a[j - 1 + m] - mu[j]) + (a[j - 1] - mu[j - 1]);
           cov += dfi * dgj + dfj * dgi;
         }
-        if (is_flat(mu[i], sig[i]) || is_flat(mu[j], sig[j])) continue;
+        if (flat[i] || flat[j]) continue;
         double corr = cov / (m * sig[i] * sig[j]);
         if (corr > cb[i] || (corr == cb[i] && j < ci[i])) { cb[i] = corr; ci[i] = j; }
         if (corr > cb[j] || (corr == cb[j] && i < ci[j])) { cb[j] = corr; ci[j] = i; }
@@ -215,6 +208,7 @@ void orc_mp(const double* a, int64_t n, int m, double* mp, int64_t* mpi) {
     mp[i] = sqrt(d2 > 0 ? d2 : 0.0);
   }
   free(corr_best);
+  free(flat);
   free(mu);
   free(sig);
 }
@@ -340,11 +334,6 @@ static void znorm(const orc_ctx* c, int64_t i, double* z) {
   for (int k = 0; k < c->m; ++k) z[k] = (c->a[i + k] - c->mu[i]) / c->sig[i];
 }
 
-/* Clipped envelope of z-normalised subsequence i (subs_U / subs_L). */
-static void sub_envelope(const orc_ctx* c, const double* z, double* lo, double* up) {
-  orc_envelope(z, c->m, c->w, lo, up);
-}
-
 /* fast bound (diag_fast): env = row r, query = column q, cross term X */
 static double fast_lb(const orc_ctx* c, int64_t r, double X) {
   double S = 2.0 * c->m + c->N[r] - 2.0 * X;
@@ -387,51 +376,112 @@ static int better(double d2, int64_t i, int64_t j, const best_t* b) {
   return (i < b->i) || (i == b->i && j < b->j);
 }
 
+/* Clipped envelope of z-normalised window j, the reference's subs_U/subs_L
+ * (lower_upper_lemire on each subsequence, new_dtw_motifGUI.cpp:37-46):
+ * lo[k] = min z_j[max(0, k-w) .. min(m-1, k+w)].  Because z = (a - mu) * isg
+ * is monotone in a, the minimum of z is z of the minimum of a: positions
+ * w <= k <= m-1-w read the raw-series envelope of radius w, the first and
+ * last w positions take running extremes over the window.  Scaled by the
+ * reciprocal deviation (LB_Keogh is a bound; the 1e-9 slack covers the last
+ * bits). */
+static void window_envelope(const orc_ctx* c, int64_t j, double* lo, double* up) {
+  const int m = c->m, w = c->w;
+  const double mu = c->mu[j], is = c->isg[j];
+  const double* x = c->a + j;
+  if (2 * w >= m - 1) { /* band covers most of the window: direct */
+    for (int k = 0; k < m; ++k) {
+      int k0 = k - w > 0 ? k - w : 0, k1 = k + w < m - 1 ? k + w : m - 1;
+      double mn = x[k0], mx = x[k0];
+      for (int t = k0 + 1; t <= k1; ++t) { mn = fmin(mn, x[t]); mx = fmax(mx, x[t]); }
+      lo[k] = (mn - mu) * is;
+      up[k] = (mx - mu) * is;
+    }
+    return;
+  }
+  for (int k = w; k <= m - 1 - w; ++k) {
+    lo[k] = (c->L[j + k] - mu) * is;
+    up[k] = (c->U[j + k] - mu) * is;
+  }
+  double mn = x[0], mx = x[0];
+  for (int t = 1; t < w; ++t) { mn = fmin(mn, x[t]); mx = fmax(mx, x[t]); }
+  for (int k = 0; k < w; ++k) {
+    mn = fmin(mn, x[k + w]); mx = fmax(mx, x[k + w]);
+    lo[k] = (mn - mu) * is;
+    up[k] = (mx - mu) * is;
+  }
+  mn = x[m - 1]; mx = x[m - 1];
+  for (int t = m - w; t < m - 1; ++t) { mn = fmin(mn, x[t]); mx = fmax(mx, x[t]); }
+  for (int k = m - 1; k >= m - w; --k) {
+    mn = fmin(mn, x[k - w]); mx = fmax(mx, x[k - w]);
+    lo[k] = (mn - mu) * is;
+    up[k] = (mx - mu) * is;
+  }
+}
+
 /* One candidate pair through Kim -> Keogh x2 -> DTW.  Returns squared DTW or
- * ORC_INF.  stage: 0 pruned by kim, 1 by keogh, 2 dtw evaluated. */
+ * ORC_INF.  stage: 0 pruned by kim, 1 by keogh, 2 dtw evaluated.
+ * LB_KK (lb_keogh.cpp:9-72): the three end terms of each side against the
+ * endpoint bound, then the middle terms with an early exit once the sum
+ * passes the threshold; the surviving direction with the larger bound gives
+ * the per-position terms whose suffix sums abandon the DTW
+ * (new_dtw_motifGUI.cpp:508-547). */
 static double eval_pair(const orc_ctx* c, int64_t i, int64_t j, double lbm, double bsf2,
                         double* buf, int* stage) {
   const int m = c->m, w = c->w;
-  double *zi = buf, *zj = buf + m, *li = buf + 2 * m, *ui = buf + 3 * m;
-  double *lj = buf + 4 * m, *uj = buf + 5 * m, *cb1 = buf + 6 * m, *cb2 = buf + 7 * m;
-  double* cb = buf + 8 * m; /* m + w + 2 */
+  double *zi = buf, *zj = buf + m, *lo = buf + 2 * m, *up = buf + 3 * m;
+  double *cb1 = buf + 4 * m, *cb2 = buf + 5 * m, *cb = buf + 6 * m; /* m + w + 2 */
+  double *prev = buf + 7 * m + w + 4, *cur = prev + m + 2;
   double thr = bsf2 * (1.0 + REL_SLACK);
-  znorm(c, i, zi);
-  znorm(c, j, zj);
+  /* endpoint bound from the three samples at each end, normalised as znorm */
+  double qi[6], tj[6];
+  for (int k = 0; k < 3; ++k) {
+    qi[k] = (c->a[i + k] - c->mu[i]) / c->sig[i];
+    tj[k] = (c->a[j + k] - c->mu[j]) / c->sig[j];
+    qi[5 - k] = (c->a[i + m - 1 - k] - c->mu[i]) / c->sig[i];
+    tj[5 - k] = (c->a[j + m - 1 - k] - c->mu[j]) / c->sig[j];
+  }
   double kl, kr;
-  orc_kim2(zi, zj, m, &kl, &kr);
+  orc_kim2(qi, tj, 6, &kl, &kr);
   if (kl + kr + lbm * lbm > thr) { *stage = 0; return ORC_INF; }
-  sub_envelope(c, zj, lj, uj);
-  sub_envelope(c, zi, li, ui);
-  /* LB_KK: endpoint Keogh terms vs the endpoint bound, then the middle */
   double lbk[2];
   for (int dir = 0; dir < 2; ++dir) {
-    const double* q = dir == 0 ? zi : zj;
-    const double* lo = dir == 0 ? lj : li;
-    const double* up = dir == 0 ? uj : ui;
+    const int64_t qw = dir == 0 ? i : j, ew = dir == 0 ? j : i;
     double* cbx = dir == 0 ? cb1 : cb2;
+    window_envelope(c, ew, lo, up);
+    const double mq = c->mu[qw], iq = c->isg[qw];
+    const double* xq = c->a + qw;
     double ends = 0.0;
-    for (int k = 0; k < m; ++k) {
-      double d = 0.0;
-      if (q[k] > up[k]) d = sq(q[k] - up[k]);
-      else if (q[k] < lo[k]) d = sq(q[k] - lo[k]);
-      cbx[k] = d;
-      if (k < KIM_BIAS || k >= m - KIM_BIAS) ends += d;
+    for (int h = 0; h < 2 * KIM_BIAS; ++h) {
+      int k = h < KIM_BIAS ? h : m - 2 * KIM_BIAS + h;
+      double v = (xq[k] - mq) * iq, d = 0.0;
+      if (v > up[k]) d = sq(v - up[k]);
+      else if (v < lo[k]) d = sq(v - lo[k]);
+      ends += d;
+      cbx[k] = 0.0;
     }
     double dist = ends > kl + kr ? ends : kl + kr;
-    for (int k = KIM_BIAS; k < m - KIM_BIAS; ++k) dist += cbx[k];
-    for (int k = 0; k < KIM_BIAS; ++k) { cbx[k] = 0.0; cbx[m - 1 - k] = 0.0; }
+    int k;
+    for (k = KIM_BIAS; k < m - KIM_BIAS; ++k) {
+      double v = (xq[k] - mq) * iq, d = 0.0;
+      if (v > up[k]) d = sq(v - up[k]);
+      else if (v < lo[k]) d = sq(v - lo[k]);
+      cbx[k] = d;
+      dist += d;
+      if (dist > thr) break;
+    }
+    if (k < m - KIM_BIAS) { *stage = 1; return ORC_INF; }
     cbx[0] = kl;
     cbx[m - KIM_BIAS] = kr;
     lbk[dir] = dist;
-    if (dist > thr) { *stage = 1; return ORC_INF; }
   }
   const double* src = lbk[0] > lbk[1] ? cb1 : cb2;
   for (int k = m; k < m + w + 2; ++k) cb[k] = 0.0;
   cb[m - 1] = src[m - 1];
   for (int k = m - 2; k >= 0; --k) cb[k] = cb[k + 1] + src[k];
+  znorm(c, i, zi);
+  znorm(c, j, zj);
   *stage = 2;
-  return orc_dtw2_ea(zi, zj, cb, m, w, thr);
+  return dtw2_rows(zi, zj, cb, m, w, thr, prev, cur);
 }
 
 double orc_pair_dist(const double* a, int64_t n, int m, int w, int64_t i, int64_t j) {
@@ -580,7 +630,7 @@ int orc_join(const double* a, int64_t n, int m, int w, unsigned flags, int threa
   uint64_t n_pairs = 0, n_fast = 0, n_masked = 0, n_kim = 0, n_keogh = 0, n_dtw = 0, n_ab = 0;
 #pragma omp parallel reduction(+ : n_pairs, n_fast, n_masked, n_kim, n_keogh, n_dtw, n_ab)
   {
-    double* buf = (double*)malloc(sizeof(double) * (size_t)(9 * m + w + 4));
+    double* buf = (double*)malloc(sizeof(double) * (size_t)(9 * m + w + 12));
 #pragma omp for schedule(dynamic, 8)
     for (int64_t L = m; L < s; ++L) {
       /* raw cross sums along the diagonal, re-anchored every 512 rows:

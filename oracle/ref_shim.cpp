@@ -13,6 +13,10 @@
 //   ref_mpx       -> mpx_v2                 CPU_version1/mpx_v2.cpp:13
 //   ref_load      -> loadfile / loadfile_apart / loadfile_2 / loadfile_
 //                                           CPU_version1/loadfile.cpp:14,35,63,114
+//   ref_mask      -> compute_shared_data_global + compute_MASK_global
+//                                           CPU_version1/compute_shared_data_global.cpp:12,
+//                                           CPU_version1/compute_MASK_global.cpp:10
+//                    with the set-up of new_dtw_motifGUI.cpp:29-45,155-207
 #include "alldef/matrix.h"
 #include "alldef/allstruct.h"
 #include "allunder/underdtw.h"
@@ -27,6 +31,14 @@
 #include <chrono>
 
 RETURN_MPX mpx_v2(const vector<DOUBLE>& timeSeries, int minlag, int subseqlen);
+void compute_shared_data_global(const vector<DOUBLE>& ts, int subseqLen,
+                                const vector<vector<DOUBLE>>& my_subs, int len_of_table_global,
+                                vector<vector<DOUBLE>>& count_table_global);
+void compute_MASK_global(const vector<DOUBLE>& a, int subseqLen,
+                         const vector<vector<DOUBLE>>& my_subs, int len_of_table_global,
+                         vector<vector<DOUBLE>>& count_table_global,
+                         const vector<vector<DOUBLE>>& subs_U, const vector<vector<DOUBLE>>& subs_L,
+                         vector<DOUBLE>& MASK_global);
 vector<DOUBLE> loadfile(string filename);
 vector<DOUBLE> loadfile_apart(string filename, int apart);
 vector<DOUBLE> loadfile_2(string filename1, string filename2);
@@ -144,6 +156,40 @@ int ref_join(const double* x, long n, int m, int w, const char* timefile,
     }
     *dist_full = std::sqrt(MON_dtw(q, t, cb, m, w, 1e300));
   }
+  return 0;
+}
+
+// The reference's global mask of series a (n samples, windows m, band w), set
+// up as new_dtw_motifGUI does: mvmean statistics, z-normalised subsequences
+// and their lower_upper_lemire envelopes (:29-45), the CDF table length from
+// the largest |z| (:155-197), then the two reference functions (:201-207).
+// Writes mask[n] (0/1) and the table length; returns 0.
+int ref_mask(const double* x, long n, int m, int w, double* mask, int* table_len) {
+  std::vector<double> a(x, x + n);
+  const long s = n - m + 1;
+  std::vector<double> mu(s), sig(s);
+  mvmean(a, m, mu, sig);
+  vector<vector<DOUBLE>> subs((size_t)s, vector<DOUBLE>(m)), U((size_t)s, vector<DOUBLE>(m)),
+      L((size_t)s, vector<DOUBLE>(m));
+  DOUBLE vmax = 0, vmin = 0;
+  for (long i = 0; i < s; ++i) {
+    for (int j = 0; j < m; ++j) subs[i][j] = (a[i + j] - mu[i]) / sig[i];
+    lower_upper_lemire(subs[i], m, w, L[i], U[i]);
+  }
+  vmax = vmin = subs[0][0];
+  for (const auto& r : subs)
+    for (auto v : r) {
+      if (v > vmax) vmax = v;
+      if (v < vmin) vmin = v;
+    }
+  DOUBLE mrv = floor(MAX(std::abs(vmax), std::abs(vmin))) * 2 * 100;
+  int lt = static_cast<int>(MAX(INITIAL_LEN_OF_TABLE, mrv));
+  vector<vector<DOUBLE>> table((size_t)m, vector<DOUBLE>((size_t)lt, 0.0));
+  compute_shared_data_global(a, m, subs, lt, table);
+  vector<DOUBLE> M((size_t)n, 0.0);
+  compute_MASK_global(a, m, subs, lt, table, U, L, M);
+  for (long p = 0; p < n; ++p) mask[p] = M[p];
+  *table_len = lt;
   return 0;
 }
 

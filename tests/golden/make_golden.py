@@ -19,7 +19,8 @@ Writes
                          MON_dtw on that pair reproduces the printed distance
   kat.json               component known answers from the reference:
                          MON_dtw on random z-normalised pairs, the clipped
-                         envelope (lower_upper_lemire), mvmean, mpx_v2
+                         envelope (lower_upper_lemire), mvmean, mpx_v2, and
+                         the global CDF mask (compute_MASK_global)
 Needs the reference sources (only on the machine that builds the fixtures).
 """
 from __future__ import annotations
@@ -60,6 +61,11 @@ CASES = [
     ("rw6k_m100_w52", "rw", 6000, 18, 100, 52),
     ("rw7k_m512_w26", "rw", 7000, 19, 512, 26),
 ]
+
+
+# global-mask known answers: (kind, n, seed, m, w)
+MASK_CASES = [("rw", 3000, 21, 64, 5), ("rw", 5000, 3, 128, 13), ("ecg", 4000, 7, 100, 10),
+              ("rw", 8000, 9, 256, 26)]
 
 
 def _oracle_brute(x, m, w):
@@ -147,9 +153,22 @@ def main():
     mpi = np.empty(x.size - m + 1, dtype=np.int32)
     ref.ref_mpx(x.ctypes.data_as(P), ctypes.c_long(x.size), m, mp.ctypes.data_as(P),
                 mpi.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    # the global CDF mask (compute_shared_data_global + compute_MASK_global,
+    # set up as new_dtw_motifGUI does) on seeded series: the positions where
+    # the mask is 1, and the CDF table length
+    masks = []
+    for kind, n, seed, mm, ww in MASK_CASES:
+        xs = synth.random_walk(n, seed) if kind == "rw" else synth.ecg_like(n, seed)
+        out = np.empty(n)
+        lt = ctypes.c_int()
+        rc = ref.ref_mask(xs.ctypes.data_as(P), ctypes.c_long(n), mm, ww, out.ctypes.data_as(P),
+                          ctypes.byref(lt))
+        assert rc == 0
+        masks.append(dict(kind=kind, n=n, seed=seed, m=mm, w=ww, table_len=lt.value,
+                          ones=np.flatnonzero(out == 1.0).tolist()))
     kat = dict(dtw=dtw, envelope_series_seed=21, envelope_n=3000, envelope=env,
                mvmean=dict(m=m, mu=mu.tolist(), sig=sg.tolist()),
-               mpx=dict(m=m, mp=mp.tolist(), mpi_1based=mpi.tolist()))
+               mpx=dict(m=m, mp=mp.tolist(), mpi_1based=mpi.tolist()), mask=masks)
     with open(os.path.join(HERE, "kat.json"), "w") as f:
         json.dump(kat, f)
     print("wrote", len(joins), "joins and kat.json")

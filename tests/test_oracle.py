@@ -88,3 +88,15 @@ def test_exact_duplicate_resolves_to_lowest_index(oracle, synth):
     r = oracle.join(x, 80, 4)
     assert r.dist == 0.0
     assert (r.i, r.j) == (400, 1200)
+
+
+def test_mask_matches_reference_mask_global(oracle, synth, kat):
+    # the global CDF mask (compute_shared_data_global + compute_MASK_global,
+    # CPU_version1/compute_MASK_global.cpp:10-92): table length and every
+    # position equal to the reference's own
+    for c in kat["mask"]:
+        x = synth.random_walk(c["n"], c["seed"]) if c["kind"] == "rw" else \
+            synth.ecg_like(c["n"], c["seed"])
+        mask, lt = oracle.mask(x, c["m"], c["w"])
+        assert lt == c["table_len"]
+        assert np.array_equal(np.flatnonzero(mask == 1.0), np.array(c["ones"])), c
