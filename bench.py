@@ -21,8 +21,10 @@ series (8 MB) and the per-series arrays (~250 MB) are re-read from HBM on
 every join; the sweep's working set far exceeds what one join leaves in L2.
 
 --impl reference times the reference's own CPU implementation (CPU_version1,
-built from its sources into oracle/_ref/) on bounded samples of the same
-series, one single-threaded process per host core.
+built from its sources into oracle/_ref/) on bounded 16,384-sample slices of
+the same series, one single-threaded process per physical host core, by the
+reference's own join interval; its line names the slices in config.workload
+and extrapolates the single-core time of the full series.
 """
 from __future__ import annotations
 
@@ -155,16 +157,43 @@ def _barrier(dist):
         dist.barrier()
 
 
+def host_cpu():
+    """(model name, physical cores available to this process)."""
+    model, cores_per_socket, sockets = "unknown", None, None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=30).stdout
+        for line in out.splitlines():
+            k, _, v = line.partition(":")
+            k, v = k.strip(), v.strip()
+            if k == "Model name":
+                model = v
+            elif k == "Core(s) per socket":
+                cores_per_socket = int(v)
+            elif k == "Socket(s)":
+                sockets = int(v)
+    except (OSError, ValueError, subprocess.TimeoutExpired):
+        pass
+    avail = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    phys = cores_per_socket * sockets if cores_per_socket and sockets else avail
+    return model, max(1, min(avail, phys))
+
+
 def cpu_sample_reference(x: np.ndarray, m: int, w: int, n_sample: int, procs: int):
-    """Runs the reference CPU join (oracle/_ref/ref_join) on `procs` disjoint
-    samples of length n_sample in parallel; returns (pairs/s, per-run info)."""
+    """Runs the reference CPU join (oracle/_ref/ref_join, CPU_version1's
+    DTWMotifDiscoveryGUI) on `procs` disjoint n_sample-long slices of x at
+    once, one single-threaded process each.  The rate of a process is its
+    slice's pairs over the reference's own join interval (the clock() time it
+    appends to its time file, CPU_version1/new_dtw_motifGUI.cpp:298,577-584:
+    the sweep after mpx_v2 and the O(n m) set-up).  Returns (summed pairs/s
+    of the processes, per-process rates, pairs per slice, wall seconds)."""
     ref_bin = os.path.join(ROOT, "oracle", "_ref", "ref_join")
     if not os.path.exists(ref_bin):
         return None
     files = []
     tmp = tempfile.mkdtemp(prefix="dtwj_ref_")
+    nslices = max(1, x.size // n_sample)
     for k in range(procs):
-        lo = (k * n_sample) % max(1, x.size - n_sample)
+        lo = (k % nslices) * n_sample
         path = os.path.join(tmp, "s%d.f64" % k)
         x[lo:lo + n_sample].astype("<f8").tofile(path)
         files.append(path)
@@ -175,14 +204,21 @@ def cpu_sample_reference(x: np.ndarray, m: int, w: int, n_sample: int, procs: in
     wall = time.perf_counter() - t0
     s = n_sample - m + 1
     pairs = (s - m) * (s - m + 1) // 2
-    runs = []
+    rates = []
     for o in outs:
         try:
             line = o.strip().splitlines()[-1].replace(": -nan", ": null").replace(": nan", ": null")
-            runs.append(json.loads(line))
+            r = json.loads(line)
         except (IndexError, json.JSONDecodeError):
-            pass
-    return pairs * len(files) / wall, wall, pairs, runs
+            continue
+        if r.get("rc") == 0 and r.get("join_seconds", 0) > 0:
+            rates.append(pairs / r["join_seconds"])
+    for f in files:
+        os.unlink(f)
+    os.rmdir(tmp)
+    if not rates:
+        return None
+    return sum(rates), rates, pairs, wall
 
 
 def cpu_sample_port(x: np.ndarray, m: int, w: int, n_sample: int, threads: int):
@@ -198,15 +234,24 @@ def cpu_sample_port(x: np.ndarray, m: int, w: int, n_sample: int, threads: int):
     return r.pairs / wall, wall, r.pairs, r.threads
 
 
+def extrapolate_reference(pairs_total: int, rate_1core: float, n_sample: int):
+    """Single-core reference join time of the whole series, extrapolated
+    proportionally to the pair count from the measured per-core rate."""
+    return {"join_seconds_1core": pairs_total / rate_1core,
+            "basis": "pairs of the full series / the reference's per-core join rate "
+                     "measured on %d-sample slices" % n_sample,
+            "label": "extrapolated"}
+
+
 def run_reference_arm(args):
-    world, rank, local, dist = int(os.environ.get("WORLD_SIZE", "1")), int(
-        os.environ.get("RANK", "0")), 0, None
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     _, synth = _load_pkg()
     wl = synth.workload(args.workload)
     x, m, w = wl["series"], wl["m"], wl["w"]
-    cores = os.cpu_count() or 1
+    model, cores = host_cpu()
     n_sample = args.ref_sample
     if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_join")):
         print(json.dumps({"impl": "reference",
@@ -215,27 +260,38 @@ def run_reference_arm(args):
         return 0
     for _ in range(args.warmup):
         cpu_sample_reference(x, m, w, n_sample, cores)
-    vals, walls = [], []
+    vals, walls, per_core = [], [], []
     for _ in range(args.steps):
-        v, wall, pairs, runs = cpu_sample_reference(x, m, w, n_sample, cores)
+        v, rates, pairs, wall = cpu_sample_reference(x, m, w, n_sample, cores)
         vals.append(v)
         walls.append(wall)
-    value = sum(vals) / len(vals)
+        per_core.extend(rates)
+    value = statistics.median(vals)
+    core_rate = statistics.median(per_core)
+    n = x.size
+    s = n - m + 1
+    pairs_total = (s - m) * (s - m + 1) // 2
+    sample = ("%d single-threaded processes (one per physical core), each CPU_version1 "
+              "DTWMotifDiscoveryGUI on its own %d-sample slice of the series; pairs/s = the "
+              "slices' pairs over the reference's own join interval (clock() t1->t2, "
+              "new_dtw_motifGUI.cpp:298,577), summed over the processes; median of %d steps"
+              % (cores, n_sample, args.steps))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(walls) / len(walls),
-        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * statistics.median(walls),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded random walk + planted motif)",
-        # the same workload as the GPU arm; each step runs bounded samples of it
-        "config": {"workload": args.workload, "n": int(x.size), "m": m, "w": w,
-                   "pairs_per_join": (x.size - 2 * m + 1) * (x.size - 2 * m + 2) // 2,
-                   "l2": "inputs+working set > L2 per join", "parallelism": "single"},
+        "config": {"workload": "%s[%d-sample slices x %d]" % (args.workload, n_sample, cores),
+                   "n": n_sample, "m": m, "w": w,
+                   "pairs_per_slice": (n_sample - 2 * m + 1) * (n_sample - 2 * m + 2) // 2,
+                   "parallelism": "%d processes" % cores},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": "%d processes, each one CPU_version1 DTWMotifDiscoveryGUI "
-                                   "(mpx_v2 + join) on a %d-sample slice of the series; "
-                                   "pairs/s = the slices' pairs over the wall time"
-                                   % (cores, n_sample)},
+                         "cpu": model, "per_core": core_rate, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "full_series": dict(extrapolate_reference(pairs_total, core_rate, n_sample),
+                            workload=args.workload, n=int(n),
+                            join_seconds_all_cores=pairs_total / value),
     }
     print(json.dumps(line))
     return 0
@@ -361,18 +417,22 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        model, _ = host_cpu()
         got = cpu_sample_reference(x, m, w, args.cpu_sample, 1)
         if got is not None:
-            v, cw, p, runs = got
-            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+            v, rates, p, cw = got
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "cpu": model,
                    "sample": "first %d samples of the series, m=%d w=%d, CPU_version1 "
-                             "DTWMotifDiscoveryGUI (mpx_v2 + join), %d pairs in %.1f s"
-                             % (args.cpu_sample, m, w, p, cw)}
+                             "DTWMotifDiscoveryGUI; pairs/s = %d pairs over the reference's own "
+                             "join interval (clock() t1->t2, new_dtw_motifGUI.cpp:298,577); "
+                             "process wall time %.1f s (with mpx_v2)"
+                             % (args.cpu_sample, m, w, p, cw),
+                   "full_series": extrapolate_reference(pairs_total, v, args.cpu_sample)}
         else:
             got = cpu_sample_port(x, m, w, args.cpu_sample, 1)
             if got is not None:
                 v, cw, p, th = got
-                cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
+                cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "port", "cpu": model,
                        "sample": "first %d samples, oracle C restatement, %.1f s"
                                  % (args.cpu_sample, cw)}
     gpu_launches = int(sum(launches.values()) * args.steps)
@@ -434,7 +494,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rw1m_motif")
     ap.add_argument("--cpu-sample", type=int, default=16384)
-    ap.add_argument("--ref-sample", type=int, default=8192)
+    ap.add_argument("--ref-sample", type=int, default=16384)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()

@@ -55,7 +55,8 @@ extern "C" {
 #define DTWJ_MAX_M 63488
 
 /* flags */
-#define DTWJ_F_NO_MASKED 0x1u   /* skip the masked diagonal bound             */
+#define DTWJ_F_NO_MASKED 0x1u   /* with DTWJ_F_MASKED_CASCADE: skip the masked
+                                   diagonal bound (endpoint bound only)       */
 #define DTWJ_F_NO_SEED 0x2u     /* no ED-profile seeding of the best-so-far   */
 #define DTWJ_F_NO_DIAG 0x4u     /* skip all diagonal bounds (LB_Keogh + DTW)  */
 #define DTWJ_F_LEARNED 0x8u     /* sweep tiles in the order the context's MLP
@@ -65,6 +66,12 @@ extern "C" {
 #define DTWJ_F_NO_GRAPH 0x40u   /* launch the sweep directly, not as a CUDA graph
                                    (by default a context captures the sweep once and
                                    replays it while its launches are unchanged) */
+#define DTWJ_F_MASKED_CASCADE 0x80u /* run filter = the reference's masked diagonal
+                                   bound and endpoint bound (diag_mask_global,
+                                   CPU_version1/diag_mask_global.cpp:11-311) on
+                                   runs of the fast bound's survivors, instead of
+                                   the default block-mean LB_Keogh bound; the
+                                   same result, more pairs reach LB_Keogh      */
 
 /* phases reported in dtwj_result.phase_seconds / phase_launches */
 #define DTWJ_PHASE_PREP 0       /* statistics, envelopes, mask, row terms     */
@@ -73,7 +80,9 @@ extern "C" {
 #define DTWJ_PHASE_DIAG 3       /* diagonal bound sweep                       */
 #define DTWJ_PHASE_PAIRS 4      /* LB_Keogh with cumulative bound + DTW       */
 #define DTWJ_PHASE_VERIFY 5     /* FP64 re-verification                       */
-#define DTWJ_PHASE_RUNS 6       /* masked / endpoint bounds on runs           */
+#define DTWJ_PHASE_RUNS 6       /* run filter: block-mean bound + endpoint bound
+                                   (or the masked cascade) on the fast bound's
+                                   survivors                                  */
 #define DTWJ_PHASE_KEOGH 7      /* LB_Keogh on the run filter's survivors     */
 #define DTWJ_NUM_PHASES 8
 
@@ -97,6 +106,7 @@ typedef struct {
   int32_t m, w;
   double phase_seconds[8];   /* with DTWJ_F_PROFILE: device time per phase   */
   uint64_t phase_launches[8];/* kernel launches per phase                    */
+  uint64_t pruned_paa;     /* pruned by the block-mean LB_Keogh bound (LB_PAA) */
 } dtwj_result;
 
 typedef struct dtwj_ctx dtwj_ctx;
@@ -123,8 +133,22 @@ int dtwj_ctx_join_device(dtwj_ctx* ctx, const double* x_dev, int64_t n, int32_t 
 /* z-normalised Euclidean matrix profile with exclusion zone m (mpx_v2,
  * CPU_version1/mpx_v2.cpp:13): mp[i] = min over |i-j| >= m, mpi[i] its
  * 0-based argmin (lowest index on ties; -1 and +inf when none).  mp, mpi
- * hold s = n - m + 1 entries. */
+ * hold s = n - m + 1 entries.  The FP64 recurrence finds each row's minimum
+ * to about 2^-17 relative; every partner within about 2^-16 of it is then
+ * measured directly in FP64, and the row takes the smallest (lowest partner
+ * on ties).  DTWJ_ERR_OVERFLOW if those near-minimal partners average more
+ * than 16 per row (a series of many near-identical windows). */
 int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64_t* mpi);
+
+/* The global CDF mask of the masked diagonal bound (compute_shared_data_global
+ * + compute_MASK_global, CPU_version1/compute_shared_data_global.cpp:12,
+ * CPU_version1/compute_MASK_global.cpp:10): mask[p] = 1 where the
+ * coverage-normalised CDF gap of the windows' envelopes at sample p is at
+ * most its mean over the series, else 0 (n floats).  table_len (may be NULL)
+ * receives the CDF table length, max(600, 200 floor(max |z|)).  Computed on
+ * the device exactly as DTWJ_F_MASKED_CASCADE joins use it. */
+int dtwj_global_mask(const double* x, int64_t n, int32_t m, int32_t w, float* mask,
+                     int32_t* table_len);
 
 /* Banded DTW distances of explicit pairs of subsequences of x (the exact
  * recurrence MON_dtw computes, CPU_version1/MON_DTW.cpp:20), FP32 on the
@@ -137,16 +161,21 @@ int dtwj_pair_dtw(const double* x, int64_t n, int32_t m, int32_t w, const int64_
  * latency-bound loop that cannot take cudaMalloc's implicit synchronisation).
  * No counterpart in the reference.  Everything is in device memory and owned
  * by the caller: x_dev (n doubles), pi_dev / pj_dev (count int64 window
- * indices), dist_dev (count doubles, the DTW distances; NaN for an index
- * outside [0, s)).  Work is enqueued on `stream` (a cudaStream_t; NULL is the
- * legacy default stream) and not waited for.  The only scratch, the window
- * statistics, is a fixed file-scope device array of 6.25 MiB holding at most
+ * indices), dist_dev (count doubles, the DTW distances).  Unlike
+ * dtwj_pair_dtw, which rejects the whole call with DTWJ_ERR_ARG, an index
+ * outside [0, s) is not checked on the host (the indices are device data):
+ * that pair's distance is NaN and the other pairs are computed.  w >= m is
+ * clamped to m - 1 (the full matrix); m must lie in [8, DTWJ_MAX_M].  Work is
+ * enqueued on `stream` (a cudaStream_t; NULL is the legacy default stream)
+ * and not waited for.  The only scratch, the window statistics, is a fixed
+ * file-scope device array of 6.25 MiB holding at most
  * DTWJ_NOALLOC_MAX_WINDOWS windows; larger series return DTWJ_ERR_SCRATCH.
- * The array's device address is looked up on the first call on each device,
- * with that device current, so make that first call before any stream
- * capture.  Every call shares the array, so calls that overlap on the GPU
- * (different streams, devices aside) race; it is rewritten by each call.
- * Makes no cudaMalloc / cudaFree or other allocating call. */
+ * The array's device address is looked up on every call, with the caller's
+ * device current, so it stays valid after cudaDeviceReset; the first call on
+ * a device also loads the library's device code there, so make that first
+ * call before any stream capture.  Every call shares the array, so calls that
+ * overlap on the GPU (different streams, devices aside) race; it is rewritten
+ * by each call.  Makes no cudaMalloc / cudaFree or other allocating call. */
 #define DTWJ_NOALLOC_MAX_WINDOWS 262144
 int dtwj_pair_dtw_noalloc(const double* x_dev, int64_t n, int32_t m, int32_t w,
                           const int64_t* pi_dev, const int64_t* pj_dev, int64_t count,
@@ -204,6 +233,21 @@ int dtwj_ctx_tiles(dtwj_ctx* ctx, const double* x, int64_t n, int32_t m, int32_t
  * (dist, i, j) over the world's results is the single-context result.  The
  * counters of each result cover its shard.  (0, 1) restores the whole join. */
 int dtwj_ctx_set_shard(dtwj_ctx* ctx, int32_t rank, int32_t world);
+
+/* Best-so-far exchange between the shards of one join (no counterpart in the
+ * reference).  With an exchange set and world > 1, a sharded join sweeps its
+ * tiles in `phases` groups (the same number on every shard, some possibly
+ * empty) and calls fn(user, bsf2_dev, count, stream) after each group: bsf2_dev
+ * is the context's device best-so-far (count uint32 words, the float bits of
+ * a squared DTW distance, which order like the floats) and stream the join's
+ * cudaStream_t.  The callback may enqueue on that stream work that lowers
+ * the words, e.g. an all-reduce(min) over the shards' contexts, so every
+ * shard prunes against the smallest distance any shard has found.  Any value
+ * the callback writes must be the squared DTW distance of some pair (or
+ * larger): pruning stays exact.  Every shard must pass the same phases.
+ * fn = NULL removes the exchange. */
+typedef void (*dtwj_exchange_fn)(void* user, uint32_t* bsf2_dev, int32_t count, void* stream);
+int dtwj_ctx_set_exchange(dtwj_ctx* ctx, dtwj_exchange_fn fn, void* user, int32_t phases);
 
 /* ---- Autotuning of the DTW band layout (no counterpart in the reference;
  * the reference fixes its layout at compile time with REGISTER_NUM) ----

@@ -43,6 +43,7 @@ F_LEARNED = 0x8
 F_VERBOSE = 0x10
 F_PROFILE = 0x20
 F_NO_GRAPH = 0x40
+F_MASKED_CASCADE = 0x80
 
 PHASES = ("prep", "profile", "seeds", "diag", "pairs", "verify", "runs", "keogh")
 
@@ -55,6 +56,7 @@ EXPORTS = (
     "dtwj_ctx_join",
     "dtwj_ctx_join_device",
     "dtwj_matrix_profile",
+    "dtwj_global_mask",
     "dtwj_pair_dtw",
     "dtwj_pair_dtw_noalloc",
     "dtwj_band",
@@ -75,6 +77,7 @@ EXPORTS = (
     "dtwj_time_band",
     "dtwj_ctx_set_band",
     "dtwj_ctx_set_shard",
+    "dtwj_ctx_set_exchange",
     "dtwj_load",
 )
 
@@ -114,6 +117,7 @@ class _Result(ctypes.Structure):
         ("w", ctypes.c_int32),
         ("phase_seconds", ctypes.c_double * 8),
         ("phase_launches", ctypes.c_uint64 * 8),
+        ("pruned_paa", ctypes.c_uint64),
     ]
 
 
@@ -140,6 +144,7 @@ class JoinResult:
     w: int
     phase_seconds: list
     phase_launches: list
+    pruned_paa: int
 
     @staticmethod
     def _from(r: _Result) -> "JoinResult":
@@ -173,6 +178,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dtwj_ctx_join_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, i64, i32, i32, u32,
                                          P(_Result)]
     lib.dtwj_matrix_profile.argtypes = [P(d), i64, i32, P(d), P(i64)]
+    lib.dtwj_global_mask.argtypes = [P(d), i64, i32, i32, P(ctypes.c_float), P(i32)]
     lib.dtwj_pair_dtw.argtypes = [P(d), i64, i32, i32, P(i64), P(i64), i64, i32, P(d)]
     vp = ctypes.c_void_p
     lib.dtwj_pair_dtw_noalloc.argtypes = [vp, i64, i32, i32, vp, vp, i64, i32, vp, vp]
@@ -198,6 +204,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dtwj_time_band.argtypes = [ctypes.c_int, i32, i32, i32, i32, i32, P(d)]
     lib.dtwj_ctx_set_band.argtypes = [vp, i32, i32, i32]
     lib.dtwj_ctx_set_shard.argtypes = [vp, i32, i32]
+    lib.dtwj_ctx_set_exchange.argtypes = [vp, EXCHANGE_FN, vp, i32]
     lib.dtwj_load.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, P(d), i64, P(i64)]
     lib.dtwj_ctx_tiles.argtypes = [vp, P(d), i64, i32, i32, P(i64), P(i32), f32p, P(d)]
     _lib = lib
@@ -248,6 +255,41 @@ def join_batch(series, ms, ws, flags: int = 0) -> list[JoinResult]:
     return [JoinResult._from(outs[q]) for q in range(k)]
 
 
+# void fn(void* user, uint32_t* bsf2_dev, int32_t count, void* stream)
+EXCHANGE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                               ctypes.c_void_p)
+
+
+class _DeviceWords:
+    """__cuda_array_interface__ view of count int32 words at a device address
+    (the context's best-so-far: float bits of non-negative squared distances,
+    which order like the floats and stay below 2^31)."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<i4",
+                                         "data": (ptr, False), "version": 3}
+
+
+def bsf_allreduce(words, group=None):
+    """Lowers every shard's best-so-far words (an int32 tensor of float bits)
+    to their minimum over the process group, in place."""
+    import torch.distributed as dist
+    dist.all_reduce(words, op=dist.ReduceOp.MIN, group=group)
+
+
+def make_exchange(group=None, device: int | None = None):
+    """Exchange callback for Context.set_exchange: an all-reduce(min) of the
+    best-so-far words over the group (NCCL), enqueued on the join's stream."""
+    import torch
+
+    def exchange(user, ptr, count, stream):
+        words = torch.as_tensor(_DeviceWords(ptr, count),
+                                device="cuda" if device is None else "cuda:%d" % device)
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+            bsf_allreduce(words, group)
+    return exchange
+
+
 class Context:
     """Reusable device context (keeps device buffers between joins)."""
 
@@ -289,6 +331,15 @@ class Context:
         rc = load().dtwj_ctx_set_shard(self._h, rank, world)
         if rc != OK:
             raise DtwjError(rc, "dtwj_ctx_set_shard")
+
+    def set_exchange(self, fn, phases: int = 8):
+        """Sharded joins sweep in `phases` groups and call fn(user, bsf2_ptr,
+        count, stream_ptr) after each (dtwj_ctx_set_exchange); None removes it."""
+        cb = EXCHANGE_FN(fn) if fn is not None else EXCHANGE_FN()
+        rc = load().dtwj_ctx_set_exchange(self._h, cb, None, phases if fn is not None else 0)
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_set_exchange")
+        self._exchange = cb  # the library holds the pointer: keep the thunk alive
 
     def set_band(self, w: int, C: int = 0, G: int = 0):
         """Joins with band w use the DTW layout (C cells per lane, G lanes per
@@ -347,6 +398,20 @@ def matrix_profile(x, m: int):
     if rc != OK:
         raise DtwjError(rc, "dtwj_matrix_profile")
     return mp, mpi
+
+
+def global_mask(x, m: int, w: int):
+    """(mask, table_len): the masked diagonal bound's global CDF mask (0/1 per
+    sample) and its CDF table length, computed on the device."""
+    a = _f64(x)
+    out = np.empty(a.size, dtype=np.float32)
+    lt = ctypes.c_int32()
+    rc = load().dtwj_global_mask(_dptr(a), a.size, m, w,
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                 ctypes.byref(lt))
+    if rc != OK:
+        raise DtwjError(rc, "dtwj_global_mask")
+    return out, lt.value
 
 
 def pair_dtw(x, m: int, w: int, pi, pj, precise: bool = True) -> np.ndarray:
@@ -490,7 +555,8 @@ def time_band(m: int, w: int, C: int, G: int, pairs: int = 2048, device: int = 0
     return v.value
 
 
-_COUNTERS = ("pairs", "pruned_fast", "pruned_kim", "pruned_masked", "pruned_keogh", "dtw_calls",
+_COUNTERS = ("pairs", "pruned_fast", "pruned_kim", "pruned_masked", "pruned_paa", "pruned_keogh",
+             "dtw_calls",
              "dtw_abandoned", "dtw_cells", "candidates")
 
 
@@ -513,10 +579,12 @@ def merge_results(results) -> JoinResult:
 
 
 def join_sharded(x, m: int, w: int, flags: int = 0, device: int | None = None, group=None,
-                 result_fn=None) -> JoinResult:
+                 result_fn=None, exchange_phases: int = 8) -> JoinResult:
     """One join spread over the ranks of a torch.distributed process group:
     rank r sweeps the tiles t with t % world == r on its device (default: the
-    current CUDA device) and the ranks exchange only their results (one
+    current CUDA device).  With exchange_phases > 0 the ranks lower each
+    other's best-so-far after each of that many sweep phases (an all-reduce
+    of one word, make_exchange); at the end they exchange their results (one
     all_gather of a few numbers).  result_fn(rank, world) replaces the device
     join (tests of the exchange without a GPU)."""
     import torch.distributed as dist
@@ -529,6 +597,8 @@ def join_sharded(x, m: int, w: int, flags: int = 0, device: int | None = None, g
             device = torch.cuda.current_device()
         with Context(device) as ctx:
             ctx.set_shard(rank, world)
+            if exchange_phases > 0 and world > 1:
+                ctx.set_exchange(make_exchange(group, device), exchange_phases)
             mine = ctx.join(x, m, w, flags)
     gathered = [None] * world
     dist.all_gather_object(gathered, mine.__dict__, group=group)

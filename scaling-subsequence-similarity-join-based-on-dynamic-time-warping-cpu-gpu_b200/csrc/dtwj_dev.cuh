@@ -5,30 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 namespace dtwj {
-
-// Runs a set-up step (a kernel attribute, which CUDA keeps per device) once
-// for each device a launch site is used on, also with several host threads.
-class OncePerDevice {
- public:
-  template <class F>
-  void run(F f) {
-    int d = 0;
-    cudaGetDevice(&d);
-    const unsigned long long bit = 1ull << (d & 63);
-    std::lock_guard<std::mutex> lock(mu_);
-    if (!(done_ & bit)) {
-      f();
-      done_ |= bit;
-    }
-  }
-
- private:
-  std::mutex mu_;
-  unsigned long long done_ = 0;
-};
 
 // Relative slack on squared distances for every pruning and abandoning test.
 // FP32 distances and the FP64 diagonal recurrences carry rounding error far
@@ -46,6 +23,26 @@ __device__ __forceinline__ float prune_threshold(unsigned int bsf2_bits, int m) 
 }
 __device__ __forceinline__ float prune_threshold_now(const unsigned int* bsf2, int m) {
   return prune_threshold(*(volatile const unsigned int*)bsf2, m);
+}
+
+// Whether an FP32 lower bound built from block-centered copies (LB_Keogh,
+// the block-mean bound) may prune a pair whose windows have error scale r
+// (the larger of their DevSeries::rw), against the squared threshold thr.
+// Every z-like difference such a bound forms is within dz = 16 * 2^-24 * r of
+// its exact value (the centered value, the FP32 reciprocal deviation, the
+// block offset and each FMA round once, every term bounded by a few r), so a
+// bound sum_k c_k d_k^2 with sum_k c_k <= m is within
+// 2 dz sqrt(m * bound) + m dz^2 of the exact one at bound <= thr, plus the
+// FP32 summation (at most m / 8 + 8 terms per lane, relative 2^-24 each).
+// The pair may be pruned when that error fits in the slack thr keeps above
+// the best-so-far: thr - bsf2 = (thr kSlack + kAbsSlackPerSample m) / (1 + kSlack).
+__device__ __forceinline__ bool fp32_bound_ok(float r, float thr, int m) {
+  const float fm = (float)m;
+  const float dz = r * (16.0f / 16777216.0f);
+  const float err = 2.0f * dz * sqrtf(fm * thr) + fm * dz * dz +
+                    thr * ((fm * 0.125f + 8.0f) * (1.0f / 16777216.0f));
+  const float slack = (thr * kSlack + kAbsSlackPerSample * fm) * (1.0f / (1.0f + kSlack));
+  return err <= slack;
 }
 
 // Endpoint bound width (the reference's BIAS, CPU_version1/diag_mask_global.cpp:8).
@@ -79,6 +76,9 @@ constexpr int kLbPerThread = 7;
 constexpr int kLbLags = kLbThreads * kLbPerThread;
 constexpr int kLbRows = 18 * kLbPerThread * 32;
 constexpr int kLbWords = kLbRows / 32;
+// Lags per group of the block-mean filter's work items (one lag per lane).
+constexpr int kLbGroups = kLbLags / 32;
+static_assert(kLbLags % 32 == 0, "lag groups of one warp");
 // Longest run of consecutive surviving rows the sweep emits as one item.
 constexpr int kRunMax = 256;
 // FP32 copies of the series and its envelopes are centered per block of
@@ -97,6 +97,7 @@ enum Counter {
   kDtwAbandoned,
   kDtwCells,
   kCandidates,
+  kPrunedPaa,
   kNumCounters
 };
 
@@ -139,6 +140,12 @@ struct DevSeries {
   double* cb;       // (n >> kBlkShift) + 2, block centers
   float* af;        // n, a - cb[block]
   float2* ulf;      // n, (U - cb[block], L - cb[block])
+  int paa_b;        // block length of the block-mean bound (8, 16 or 32)
+  float* pa;        // n, mean of a[p, p + paa_b) - cb[block of p]
+  float2* pul;      // n, the same means of (U, L)
+  float* cmax;      // (n >> kBlkShift) + 2, largest |centered FP32 value| per block
+  float* rw;        // s, FP32 error scale of window i: isg_i x the largest
+                    //    centered magnitude or block offset its FP32 bounds read
   int* status;      // device status word (0 ok, else error bits)
 };
 
@@ -228,6 +235,22 @@ void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
                         const unsigned long long* lo, double* mp, int64_t* mpi,
                         cudaStream_t st);
 void launch_reverse(const double* a, int64_t n, double* out, cudaStream_t st);
+// Exact profile: want / wrev = the smaller first-pass key of each row (by
+// series row / by reversed row); the collect pass lists every pair whose high
+// word is near its row's key; the exact pass computes their FP64 distance
+// (pick = false: row minima of the bits, true: lowest partner at the minimum;
+// reversed: the candidates are rows of the reversed series).
+void launch_mp_want(int64_t s, const unsigned long long* up, const unsigned long long* lo,
+                    unsigned long long* want, unsigned long long* wrev, cudaStream_t st);
+void launch_mp_collect(const DevSeries& S, const Tile* tiles, int ntiles,
+                       const unsigned long long* want, int2* cand, unsigned int* count,
+                       unsigned int cap, cudaStream_t st);
+void launch_mp_exact(const DevSeries& S, const int2* cand, const unsigned int* count,
+                     unsigned int cap, bool reversed, bool pick, unsigned long long* rowmin,
+                     unsigned long long* rowidx, cudaStream_t st);
+void launch_mp_exact_out(int64_t s, const unsigned long long* rowmin,
+                         const unsigned long long* rowidx, double* mp, int64_t* mpi,
+                         cudaStream_t st);
 // kSeeds seeds per series into seeds[series * kSeeds ...] (unused slots hold
 // (-1, -1)), their counts into nseeds[series] and the initial best-so-far
 // into bsf2[series].
@@ -255,6 +278,15 @@ void launch_center(const DevSeries& S, cudaStream_t st);
 // profile keys of the series' rows; out[64 * t ...] for tile t.
 void launch_tile_features(const DevSeries& S, const Tile* tiles, int ntiles,
                           const unsigned long long* keys, float* out, cudaStream_t st);
+// Block-mean lower bound (LB_PAA) over the survivor bits of LB tiles
+// [tile_begin, tile_end), then the endpoint bound; survivors go to Q.kq.
+void launch_paa(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
+                int tile_end, const unsigned int* bits, int num_sms, cudaStream_t st);
+// Block length of the block-mean bound for windows of length m.
+int paa_block(int m);
+// Sliding block means (pa, pul), per-block magnitudes (cmax) and per-window
+// error scales (rw); after launch_center.
+void launch_paa_prep(const DevSeries& S, cudaStream_t st);
 // LB_Keogh over the candidates the run filter queued in Q.kq; survivors go to
 // Q.queue.
 void launch_keogh(const DevSeries& S, const DevSearch& Q, int num_sms, cudaStream_t st);

@@ -19,7 +19,8 @@
 //             the smallest profile value of the tile's rows / sqrt(2m), 1
 //
 // The matrix-profile keys are those of the profile pass: high 32 bits of the
-// FP64 squared distance, low 32 bits the partner (ULLONG_MAX: none).
+// FP64 squared distance with the 3 lowest cleared, low 32 bits the partner
+// (ULLONG_MAX: none).
 #include "dtwj_dev.cuh"
 
 #include <climits>

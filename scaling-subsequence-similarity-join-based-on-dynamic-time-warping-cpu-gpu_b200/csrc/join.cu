@@ -61,6 +61,9 @@ struct dtwj_ctx {
   dtwj_mlp* model = nullptr;               // scores tiles for DTWJ_F_LEARNED (not owned)
   std::vector<std::pair<int, BandShape>> band_override;  // band w -> DTW layout (autotuner)
   int shard_rank = 0, shard_world = 1;  // this context sweeps tiles t with t % world == rank
+  dtwj_exchange_fn exchange = nullptr;  // best-so-far exchange between sweep phases
+  void* exchange_user = nullptr;
+  int exchange_phases = 0;
   std::vector<cudaEvent_t> pool;  // events for per-phase device times
   // the sweep's launches captured as a CUDA graph, replayed while every
   // launch argument is unchanged (same buffers, tiles, band, flags)
@@ -78,7 +81,8 @@ enum BufId {
   B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
   B_MP, B_MPI, B_CB, B_AF, B_ULF, B_BITS, B_LBTILES, B_KQ, B_SBEG, B_SID, B_SEEDBSF,
-  B_BEST_IJ, B_BEST_F32, B_QSER, B_TILEBEST, B_FEAT, B_SCORE,
+  B_BEST_IJ, B_BEST_F32, B_QSER, B_TILEBEST, B_FEAT, B_SCORE, B_PA, B_PUL, B_CMAX, B_RW,
+  B_MPX_WANT, B_MPX_WREV, B_MPX_MIN, B_MPX_IDX, B_MPX_CAND, B_MPX_CNT,
   B_COUNT_
 };
 
@@ -254,6 +258,11 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   ENSURE(B_CB, ((n >> kBlkShift) + 4) * 8, S.cb);
   ENSURE(B_AF, n * 4, S.af);
   ENSURE(B_ULF, n * 8, S.ulf);
+  ENSURE(B_PA, n * 4, S.pa);
+  ENSURE(B_PUL, n * 8, S.pul);
+  ENSURE(B_CMAX, ((n >> kBlkShift) + 4) * 4, S.cmax);
+  ENSURE(B_RW, s * 4, S.rw);
+  S.paa_b = paa_block(m);
   ENSURE(B_STATUS, 4, S.status);
   cudaStream_t st = ctx->stream;
   CUDA_OK(cudaMemsetAsync(S.status, 0, 4, st));
@@ -302,7 +311,8 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   }
   launch_rowterms(S, masked, st);
   launch_center(S, st);
-  if (ph) ph->end(DTWJ_PHASE_PREP, masked ? 11 : 6);
+  launch_paa_prep(S, st);
+  if (ph) ph->end(DTWJ_PHASE_PREP, masked ? 14 : 9);
   CUDA_OK(cudaGetLastError());
   *out = S;
   return DTWJ_OK;
@@ -336,7 +346,10 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   if (learned && !ctx->model) return DTWJ_ERR_NOMODEL;
   if (learned && mlp_device(ctx->model) != ctx->device) return DTWJ_ERR_ARG;
   const bool tile_mode = tq && tq->min_dist;
-  const bool masked = !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
+  // the run filter: the block-mean bound (default), or the reference's masked
+  // diagonal bound and endpoint bound (DTWJ_F_MASKED_CASCADE)
+  const bool cascade = (flags & DTWJ_F_MASKED_CASCADE) != 0;
+  const bool masked = cascade && !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
   const bool verbose = flags & DTWJ_F_VERBOSE;
   cudaStream_t st = ctx->stream;
   Phases ph(ctx, (flags & DTWJ_F_PROFILE) != 0);
@@ -490,6 +503,23 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   if (enumerate_all) chunk = (int)((double)qcap / tile_pairs) > 0 ? (int)((double)qcap / tile_pairs) : 1;
   unsigned int* bits;
   ENSURE(B_BITS, (size_t)(chunk < nlb ? chunk : (nlb > 0 ? nlb : 1)) * kLbLags * kLbWords * 4, bits);
+  // the stages after the diagonal bound of one chunk: run filter, LB_Keogh, DTW
+  auto filter_chunk = [&](int t0, int t1) {
+    ph.begin();
+    if (enumerate_all || cascade)
+      launch_runs(S, Q, lbtiles, t0, t1, bits, masked, !enumerate_all, ctx->num_sms, st);
+    else
+      launch_paa(S, Q, lbtiles, t0, t1, bits, ctx->num_sms, st);
+    ph.end(DTWJ_PHASE_RUNS, 1);
+    if (!enumerate_all) {
+      ph.begin();
+      launch_keogh(S, Q, ctx->num_sms, st);
+      ph.end(DTWJ_PHASE_KEOGH, 1);
+    }
+    ph.begin();
+    launch_pairs(S, Q, Q.queue, Q.queue_count, true, band, ctx->num_sms, st);
+    ph.end(DTWJ_PHASE_PAIRS, 1);
+  };
   // one pass over all tiles in chunks: bound sweep, run filter, LB_Keogh, DTW
   auto sweep = [&](int ch) -> int {
     for (int t0 = 0; t0 < nlb; t0 += ch) {
@@ -498,24 +528,41 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
       ph.begin();
       launch_lb(S, Q, lbtiles, t0, t1, bits, enumerate_all, lb_next, ctx->num_sms, st);
       ph.end(DTWJ_PHASE_DIAG, 1);
-      ph.begin();
-      launch_runs(S, Q, lbtiles, t0, t1, bits, masked, !enumerate_all, ctx->num_sms, st);
-      ph.end(DTWJ_PHASE_RUNS, 1);
-      if (!enumerate_all) {
+      filter_chunk(t0, t1);
+    }
+    CUDA_OK(cudaGetLastError());
+    return DTWJ_OK;
+  };
+  // a sharded join with an exchange sweeps its tiles in phases and lets the
+  // caller lower the best-so-far between them (direct launches)
+  const bool exchanging = ctx->exchange && ctx->shard_world > 1 && !tq;
+  auto sweep_phased = [&]() -> int {
+    const int P = ctx->exchange_phases;
+    for (int ph_i = 0; ph_i < P; ++ph_i) {
+      const int a = (int)((int64_t)nlb * ph_i / P), b = (int)((int64_t)nlb * (ph_i + 1) / P);
+      for (int t0 = a; t0 < b; t0 += chunk) {
+        const int t1 = t0 + chunk < b ? t0 + chunk : b;
+        CUDA_OK(cudaMemsetAsync(qc, 0, 32, st));
         ph.begin();
-        launch_keogh(S, Q, ctx->num_sms, st);
-        ph.end(DTWJ_PHASE_KEOGH, 1);
+        launch_lb(S, Q, lbtiles, t0, t1, bits, enumerate_all, lb_next, ctx->num_sms, st);
+        ph.end(DTWJ_PHASE_DIAG, 1);
+        filter_chunk(t0, t1);
       }
-      ph.begin();
-      launch_pairs(S, Q, Q.queue, Q.queue_count, true, band, ctx->num_sms, st);
-      ph.end(DTWJ_PHASE_PAIRS, 1);
+      ctx->exchange(ctx->exchange_user, Q.bsf2, nslots, (void*)st);
     }
     CUDA_OK(cudaGetLastError());
     return DTWJ_OK;
   };
   for (int attempt = 0;; ++attempt) {
     bool swept = false;
-    if (attempt == 0 && !(flags & DTWJ_F_NO_GRAPH) && nlb > 0) {
+    // only the first pass exchanges: a shard whose queues overflowed re-sweeps
+    // alone, and every shard must make the same exchange calls
+    if (exchanging && attempt == 0) {
+      const int src = sweep_phased();
+      if (src) return src;
+      swept = true;
+    }
+    if (!swept && attempt == 0 && !(flags & DTWJ_F_NO_GRAPH) && nlb > 0) {
       // the first pass runs as a CUDA graph: replayed if this context captured
       // the same launches before, captured (then launched) otherwise
       std::vector<unsigned char> key;
@@ -524,9 +571,9 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
         key.insert(key.end(), b, b + bytes);
       };
       const int band_cg[2] = {band.C, band.G};
-      const int64_t misc[9] = {nlb, chunk, enumerate_all, masked, ctx->num_sms, ph.on,
-                               (int64_t)ph.used, (int64_t)(uintptr_t)lbtiles,
-                               (int64_t)(uintptr_t)bits};
+      const int64_t misc[10] = {nlb, chunk, enumerate_all, masked, cascade, ctx->num_sms, ph.on,
+                                (int64_t)ph.used, (int64_t)(uintptr_t)lbtiles,
+                                (int64_t)(uintptr_t)bits};
       put(&S, sizeof S);
       put(&Q, sizeof Q);
       put(band_cg, sizeof band_cg);
@@ -662,6 +709,7 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
       out->pruned_kim = cnt_h[kPrunedKim];
       out->pruned_masked = cnt_h[kPrunedMasked];
       out->pruned_keogh = cnt_h[kPrunedKeogh];
+      out->pruned_paa = cnt_h[kPrunedPaa];
       out->dtw_calls = cnt_h[kDtwCalls];
       out->dtw_abandoned = cnt_h[kDtwAbandoned];
       out->dtw_cells = cnt_h[kDtwCells];
@@ -831,6 +879,14 @@ int dtwj_ctx_set_shard(dtwj_ctx* ctx, int32_t rank, int32_t world) {
   if (!ctx || world < 1 || rank < 0 || rank >= world) return DTWJ_ERR_ARG;
   ctx->shard_rank = rank;
   ctx->shard_world = world;
+  return DTWJ_OK;
+}
+
+int dtwj_ctx_set_exchange(dtwj_ctx* ctx, dtwj_exchange_fn fn, void* user, int32_t phases) {
+  if (!ctx || (fn && phases < 1)) return DTWJ_ERR_ARG;
+  ctx->exchange = fn;
+  ctx->exchange_user = fn ? user : nullptr;
+  ctx->exchange_phases = fn ? phases : 0;
   return DTWJ_OK;
 }
 
@@ -1008,7 +1064,50 @@ int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64
     double* dmp = (double*)p;
     if ((rc = ensure(ctx, B_MPI, s * 8, &p))) break;
     int64_t* dmpi = (int64_t*)p;
-    launch_mp_finalize(S, up, lo, dmp, dmpi, ctx->stream);
+    // Exact pass.  The first pass keeps about 17 mantissa bits of ED^2 per
+    // row; every pair whose key lies within ten 20-bit units of its row's
+    // smallest key (either direction) is a candidate, its FP64 distance is
+    // computed directly, and the row takes the smallest, lowest partner on
+    // ties.
+    unsigned long long *want, *wrev, *rowmin, *rowidx;
+    if ((rc = ensure(ctx, B_MPX_WANT, s * 8, &p))) break;
+    want = (unsigned long long*)p;
+    if ((rc = ensure(ctx, B_MPX_WREV, s * 8, &p))) break;
+    wrev = (unsigned long long*)p;
+    if ((rc = ensure(ctx, B_MPX_MIN, s * 8, &p))) break;
+    rowmin = (unsigned long long*)p;
+    if ((rc = ensure(ctx, B_MPX_IDX, s * 8, &p))) break;
+    rowidx = (unsigned long long*)p;
+    const unsigned int cap =
+        (unsigned int)(s * 16 + 4096 < (1ll << 31) ? s * 16 + 4096 : (1ll << 31));
+    if ((rc = ensure(ctx, B_MPX_CAND, (size_t)cap * sizeof(int2), &p))) break;
+    int2* cand_up = (int2*)p;
+    if ((rc = ensure(rev, B_MPX_CAND, (size_t)cap * sizeof(int2), &p))) break;
+    int2* cand_lo = (int2*)p;
+    if ((rc = ensure(ctx, B_MPX_CNT, 8, &p))) break;
+    unsigned int* cnt = (unsigned int*)p;
+    cudaStream_t st = ctx->stream;
+    launch_mp_want(s, up, lo, want, wrev, st);
+    cudaMemsetAsync(cnt, 0, 8, st);
+    cudaMemsetAsync(rowmin, 0xff, s * 8, st);
+    cudaMemsetAsync(rowidx, 0xff, s * 8, st);
+    launch_mp_collect(S, tiles, nlb, want, cand_up, cnt, cap, st);
+    launch_mp_collect(R, tiles, nlb, wrev, cand_lo, cnt + 1, cap, st);
+    for (int pick = 0; pick < 2; ++pick) {
+      launch_mp_exact(S, cand_up, cnt, cap, false, pick != 0, rowmin, rowidx, st);
+      launch_mp_exact(S, cand_lo, cnt + 1, cap, true, pick != 0, rowmin, rowidx, st);
+    }
+    launch_mp_exact_out(s, rowmin, rowidx, dmp, dmpi, st);
+    unsigned int cnt_h[2] = {0, 0};
+    if (cudaMemcpyAsync(cnt_h, cnt, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      rc = DTWJ_ERR_CUDA;
+      break;
+    }
+    if (cnt_h[0] > cap || cnt_h[1] > cap) {
+      rc = DTWJ_ERR_OVERFLOW;
+      break;
+    }
     if (cudaMemcpyAsync(mp, dmp, s * 8, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
         cudaMemcpyAsync(mpi, dmpi, s * 8, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
@@ -1017,6 +1116,43 @@ int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64
     }
   } while (0);
   dtwj_ctx_destroy(rev);
+  dtwj_ctx_destroy(ctx);
+  return rc;
+}
+
+int dtwj_global_mask(const double* x, int64_t n, int32_t m, int32_t w, float* mask,
+                     int32_t* table_len) {
+  if (!mask) return DTWJ_ERR_ARG;
+  int rc = check_args(x, n, m, w);
+  if (rc) return rc;
+  const int we = effective_band(m, w);
+  dtwj_ctx* ctx = nullptr;
+  rc = dtwj_ctx_create(0, &ctx);
+  if (rc) return rc;
+  do {
+    double* dev = nullptr;
+    if ((rc = upload(ctx, x, n, &dev))) break;
+    DevSeries S;
+    if ((rc = prepare(ctx, dev, n, m, we, true, nullptr, 1, &S))) break;
+    if (cudaMemcpyAsync(mask, S.mask, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      rc = DTWJ_ERR_CUDA;
+      break;
+    }
+    if (table_len) {
+      // the table length the mask used: 200 floor(max |z|), at least 600
+      float zmax = 0.0f;
+      void* p = nullptr;
+      if ((rc = ensure(ctx, B_ZMAX, 4, &p))) break;
+      if (cudaMemcpy(&zmax, p, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        rc = DTWJ_ERR_CUDA;
+        break;
+      }
+      const int lt = (int)(std::floor((double)zmax) * 200.0);
+      *table_len = lt > 600 ? lt : 600;
+    }
+  } while (0);
   dtwj_ctx_destroy(ctx);
   return rc;
 }

@@ -24,8 +24,10 @@
 // thread keeps a sliding window of its kLbPerThread columns in registers, so
 // every shared load feeds kLbPerThread pairs (kLbPerThread is odd, so the
 // strided FP64 reads are bank-conflict free).  Survivors are written as one
-// bit per pair, 32 rows per word, [tile][lag][word]; the run filter
-// (runs.cu) turns the bits back into runs of consecutive rows.
+// bit per pair, 32 rows per word, [tile][word][lag]: the kLbLags words of one
+// row word are contiguous, so a warp's seven stores of a word index fill the
+// same seven lines.  The block-mean filter (paa.cu) reads a word of 32
+// consecutive lags per warp; the run filter (runs.cu) reads one lag's words.
 #include "dtwj_dev.cuh"
 
 namespace dtwj {
@@ -142,6 +144,9 @@ __device__ __forceinline__ void lb_tile(const DevSeries& S, const DevSearch& Q, 
       ws[l] = sh.sg[cb + l];
       wg[l] = sh.g[cb + l];
     }
+    // survivor bits enter at the bottom of each lag's word (word = 2 word +
+    // bit), so after 32 rows row r of the word sits at bit 31 - r; the word is
+    // reversed and masked to the pairs that exist when it is stored
     unsigned int word[kLbPerThread];
 #pragma unroll
     for (int l = 0; l < kLbPerThread; ++l) word[l] = 0u;
@@ -149,8 +154,6 @@ __device__ __forceinline__ void lb_tile(const DevSeries& S, const DevSearch& Q, 
 #pragma unroll
       for (int u = 0; u < kLbPerThread; ++u) {
         const int r = qq * kLbPerThread + u;   // stage row; r % K == u
-        const int64_t i = r0 + r;
-        const bool row_ok = st + r < T.rows;
         const bool first = (st == 0 && r == 0);
         const double q1 = sh.r1[r], q2 = sh.r2[r], q3 = sh.r3[r], q4 = sh.r4[r];
         const double qs = sh.rs[r], qg = sh.rg[r];
@@ -163,12 +166,13 @@ __device__ __forceinline__ void lb_tile(const DevSeries& S, const DevSearch& Q, 
             Cr[l] = fma(q1, w4[sl], Cr[l]);
             Cr[l] = fma(w3[sl], q2, Cr[l]);
           }
-          const bool valid = row_ok && i + Lt + l < s;
-          // with the bounds off (best-so-far +inf) only flat windows prune
-          const bool prune = fma(qg, ws[sl], -Cf[l]) > 0.0 || fma(wg[sl], qs, -Cr[l]) > 0.0;
-          npairs += valid ? 1u : 0u;
-          nfast += (valid && prune) ? 1u : 0u;
-          word[l] |= (valid && !prune ? 1u : 0u) << (r & 31);
+          // a direction prunes when G sigma - C > 0; the sign of the high word
+          // decides (hi > 0: positive; zero, denormals and negatives survive,
+          // which only keeps more pairs).  With the bounds off (best-so-far
+          // +inf) only flat windows prune.
+          const int hf = __double2hiint(fma(qg, ws[sl], -Cf[l]));
+          const int hr = __double2hiint(fma(wg[sl], qs, -Cr[l]));
+          word[l] = word[l] * 2u + (max(hf, hr) <= 0 ? 1u : 0u);
         }
         // the column lag K-1 needs at the next row replaces the one lag 0 used
         const int nx = cb + r + kLbPerThread;
@@ -180,9 +184,18 @@ __device__ __forceinline__ void lb_tile(const DevSeries& S, const DevSearch& Q, 
         wg[u] = sh.g[nx];
         if ((r & 31) == 31) {
           const int wi = (st + r) >> 5;
+          // pairs that exist: tile row x < rows and i0 + x + Lt + l < s
+          const int64_t room = s - i0 - Lt - (int64_t)wi * 32;
+          const int64_t rows_left = (int64_t)T.rows - (int64_t)wi * 32;
 #pragma unroll
           for (int l = 0; l < kLbPerThread; ++l) {
-            out[(size_t)(t * kLbPerThread + l) * kLbWords + wi] = word[l];
+            const int64_t lim = room - l < rows_left ? room - l : rows_left;
+            const unsigned int vm =
+                lim >= 32 ? 0xffffffffu : (lim <= 0 ? 0u : (1u << (int)lim) - 1u);
+            const unsigned int wv = __brev(word[l]) & vm;
+            npairs += __popc(vm);
+            nfast += __popc(vm & ~wv);
+            out[(size_t)wi * kLbLags + t * kLbPerThread + l] = wv;
             word[l] = 0u;
           }
         }
@@ -192,7 +205,7 @@ __device__ __forceinline__ void lb_tile(const DevSeries& S, const DevSearch& Q, 
   // words past the tile's last stage (short tiles) are zero, never stale
   for (int wi = ((T.rows + kStage - 1) / kStage) * (kStage / 32); wi < kLbWords; ++wi) {
 #pragma unroll
-    for (int l = 0; l < kLbPerThread; ++l) out[(size_t)(t * kLbPerThread + l) * kLbWords + wi] = 0u;
+    for (int l = 0; l < kLbPerThread; ++l) out[(size_t)wi * kLbLags + t * kLbPerThread + l] = 0u;
   }
 }
 
@@ -235,10 +248,7 @@ void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int ti
                int tile_end, unsigned int* bits, bool enumerate_all, unsigned int* next,
                int num_sms, cudaStream_t st) {
   if (tile_end <= tile_begin) return;
-  static OncePerDevice setup;
-  setup.run([] {
-    cudaFuncSetAttribute(k_lb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LbShared));
-  });
+  cudaFuncSetAttribute(k_lb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LbShared));
   const int ntiles = tile_end - tile_begin;
   const int resident = 3 * num_sms;  // three CTAs per SM (launch bounds, 64.5 KB shared each)
   k_lb<<<ntiles < resident ? ntiles : resident, kLbThreads, sizeof(LbShared), st>>>(

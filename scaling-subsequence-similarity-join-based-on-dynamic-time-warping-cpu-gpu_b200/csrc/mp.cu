@@ -10,9 +10,11 @@
 // re-anchored exactly at the first row of every tile, and the row minimum of
 // ED^2 = 2m - 2 C / (sig_i sig_j) is reduced across the warp in one REDUX.
 // A key packs the high 32 bits of ED^2 (sign, exponent, 20 mantissa bits:
-// monotone for non-negative doubles) above the partner index, so a 64-bit
-// atomicMin keeps the nearest neighbour with the lowest index on ties at that
-// resolution; the finalize pass recomputes the exact FP64 distance.
+// monotone for non-negative doubles; the lowest 3 bits give way to the lag
+// inside a thread's minimum) above the partner index, so a 64-bit atomicMin
+// keeps the nearest neighbour at that resolution.  That is all the seeds
+// need; the matrix profile (dtwj_matrix_profile) then decides every row at
+// FP64 among the partners whose key is near the row's (launch_mp_collect).
 //
 // The seeds are the kSeeds smallest row minima, as in
 // CPU_version1/new_dtw_motifGUI.cpp:53-74 (min_v_k + exact DTW per seed).
@@ -34,15 +36,32 @@ namespace {
 constexpr int kStage = kLbPerThread * 32;
 constexpr int kCols = kLbLags + kStage;
 
+// High words of ED^2 keys at or above this (ED^2 >= 2^513) come from the
+// 1e300 offset of a column past the series or of a flat window, not a pair.
+constexpr unsigned int kKeyReal = 0x60000000u;
+static_assert(kLbPerThread <= 8, "the lag fits the key's 3 low bits");
+
 struct MpShared {
   double p1[kCols], p2[kCols], is[kCols], c2[kCols];
   double r1[kStage], r2[kStage], ci[kStage];
+  unsigned int lim[kStage];
   unsigned long long rowbest[kLbRows];
 };
 
+// Candidate list of the exact profile (COLLECT): every pair whose high word
+// is within ten units of its row's smallest key.
+struct MpCollect {
+  const unsigned long long* want;  // per row: the smallest key of the first pass
+  int2* cand;
+  unsigned int* count;
+  unsigned int cap;
+};
+
+template <bool COLLECT>
 __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* tiles,
                                                       unsigned long long* keys,
-                                                      unsigned int* tile_best, int tile_base) {
+                                                      unsigned int* tile_best, int tile_base,
+                                                      MpCollect col) {
   extern __shared__ __align__(16) unsigned char smraw[];
   MpShared& sh = *reinterpret_cast<MpShared*>(smraw);
   const Tile T = tiles[blockIdx.x];
@@ -94,6 +113,12 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
       sh.r1[x] = up ? S.dfa[i - 1] : 0.0;
       sh.r2[x] = up ? S.dga[i - 1] : 0.0;
       sh.ci[x] = (in && !S.flat[i]) ? -2.0 * S.isg[i] : 0.0;
+      if (COLLECT) {
+        // the first pass's key is the row's smallest high word with its 3
+        // low bits cleared: its partners lie within 8 units, plus 2 of margin
+        const unsigned long long k = in ? col.want[i] : ULLONG_MAX;
+        sh.lim[x] = k == ULLONG_MAX ? 0u : (unsigned int)(k >> 32) + 10u;
+      }
     }
     __syncthreads();
     const int cb = t * kLbPerThread;
@@ -111,8 +136,12 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
         const int64_t i = r0 + r;
         const bool first = (st == 0 && r == 0);
         const double q1 = sh.r1[r], q2 = sh.r2[r], qc = sh.ci[r];
+        const unsigned int lim = COLLECT ? sh.lim[r] : 0u;
+        // rows of the tile with a non-flat window (warp-uniform); a column past
+        // the series or flat has weight 0 and offset 1e300, so its key is far
+        // above any real one and it never needs a test of its own
+        const bool row_ok = (st + r < T.rows) && qc != 0.0;
         unsigned int best = UINT_MAX;
-        int bl = 0;
 #pragma unroll
         for (int l = 0; l < kLbPerThread; ++l) {
           const int sl = (u + l) % kLbPerThread;
@@ -122,10 +151,15 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
           }
           const double e2 = fmax(fma(C[l] * qc, wi[sl], wc[sl]), 0.0);
           const unsigned int hi = (unsigned int)__double2hiint(e2);
-          const bool ok = (st + r < T.rows) && (i + Lt + l < s);
-          if (ok && hi < best) {
-            best = hi;
-            bl = l;
+          if (COLLECT) {
+            if (row_ok && hi <= lim) {
+              const unsigned int slot = atomicAdd(col.count, 1u);
+              if (slot < col.cap) col.cand[slot] = make_int2((int)i, (int)(i + Lt + l));
+            }
+          } else {
+            // the high word with its lowest 3 bits replaced by the lag: one
+            // minimum keeps the nearest lag (17 mantissa bits of ED^2)
+            best = min(best, (hi & ~7u) | (unsigned int)l);
           }
         }
         const int nx = cb + r + kLbPerThread;
@@ -133,13 +167,14 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
         w2[u] = sh.p2[nx];
         wi[u] = sh.is[nx];
         wc[u] = sh.c2[nx];
-        if (qc != 0.0) {  // flat rows have no neighbour
+        if (!COLLECT && row_ok) {  // flat rows have no neighbour
           const unsigned int wbest = __reduce_min_sync(0xffffffffu, best);
-          if (wbest != UINT_MAX) {
+          if (wbest < kKeyReal) {
             const unsigned int ballot = __ballot_sync(0xffffffffu, best == wbest);
             if (lane == __ffs(ballot) - 1) {
               const unsigned long long key =
-                  ((unsigned long long)wbest << 32) | (unsigned long long)(unsigned int)(i + Lt + bl);
+                  ((unsigned long long)(wbest & ~7u) << 32) |
+                  (unsigned long long)(unsigned int)(i + Lt + (wbest & 7u));
               atomicMin(&sh.rowbest[st + r], key);
             }
           }
@@ -147,6 +182,7 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
       }
     }
   }
+  if (COLLECT) return;
   __syncthreads();
   unsigned int tmin = 0xffffffffu;  // the tile's smallest key (high bits of ED^2)
   for (int x = t; x < T.rows; x += kLbThreads) {
@@ -172,7 +208,9 @@ __global__ void k_tile_bound(const unsigned int* tile_best, int ntiles, unsigned
     bsf2[t] = 0x7f800000u;
     return;
   }
-  const unsigned long long bits = ((unsigned long long)hi + 1ull) << 32;
+  // the key's high word has its 3 low bits cleared: the pair's ED^2 is below
+  // the next multiple of 8 units
+  const unsigned long long bits = ((unsigned long long)(hi & ~7u) + 8ull) << 32;
   bsf2[t] = __float_as_uint(__double2float_ru(__longlong_as_double((long long)bits)));
 }
 
@@ -212,6 +250,64 @@ __global__ void k_mp_finalize(DevSeries S, const unsigned long long* up,
   }
   mp[i] = sqrt(d2);
   mpi[i] = j;
+}
+
+// Exact squared distance of candidate pairs, one warp per pair (the same
+// arithmetic as k_mp_finalize).  A candidate (i, j) of the reversed series is
+// the pair (s-1-i, s-1-j) of the series.  pick == false: rowmin[i] = the
+// smallest FP64 bits over the row's candidates (non-negative doubles order as
+// their bits); pick == true: rowidx[i] = the lowest partner reaching it.
+__global__ void k_mp_exact(DevSeries S, const int2* cand, const unsigned int* count,
+                           unsigned int cap, bool reversed, bool pick,
+                           unsigned long long* rowmin, unsigned long long* rowidx) {
+  const int lane = threadIdx.x & 31;
+  const unsigned int total = *count < cap ? *count : cap;
+  for (unsigned int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < total;
+       c += (gridDim.x * blockDim.x) >> 5) {
+    const int2 p = cand[c];
+    const int64_t i = reversed ? S.s - 1 - p.x : p.x, j = reversed ? S.s - 1 - p.y : p.y;
+    const double mi = S.mu[i], mj = S.mu[j], si = S.isg[i], sj = S.isg[j];
+    double d2 = 0.0;
+    for (int q = lane; q < S.m; q += 32) {
+      const double d = (S.a[i + q] - mi) * si - (S.a[j + q] - mj) * sj;
+      d2 = fma(d, d, d2);
+    }
+    for (int o = 16; o > 0; o >>= 1) d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+    if (lane == 0) {
+      const unsigned long long b = (unsigned long long)__double_as_longlong(d2);
+      if (!pick) atomicMin(&rowmin[i], b);
+      else if (b == rowmin[i]) atomicMin(&rowidx[i], (unsigned long long)j);
+    }
+  }
+}
+
+// mp[i] = sqrt of the row's exact minimum, mpi[i] its lowest partner.
+__global__ void k_mp_exact_out(int64_t s, const unsigned long long* rowmin,
+                               const unsigned long long* rowidx, double* mp, int64_t* mpi) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= s) return;
+  if (rowidx[i] == ULLONG_MAX) {
+    mp[i] = __longlong_as_double(0x7ff0000000000000LL);
+    mpi[i] = -1;
+    return;
+  }
+  mp[i] = sqrt(__longlong_as_double((long long)rowmin[i]));
+  mpi[i] = (int64_t)rowidx[i];
+}
+
+// want[i] = the smaller of row i's keys over j > i (up) and over j < i (lo,
+// rows of the reversed series); wrev is the same indexed by reversed rows.
+__global__ void k_mp_want(int64_t s, const unsigned long long* up, const unsigned long long* lo,
+                          unsigned long long* want, unsigned long long* wrev) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= s) return;
+  const unsigned long long a = up[i], b = lo[s - 1 - i];
+  const unsigned long long ha = a == ULLONG_MAX ? ULLONG_MAX : (a >> 32);
+  const unsigned long long hb = b == ULLONG_MAX ? ULLONG_MAX : (b >> 32);
+  const unsigned long long h = ha < hb ? ha : hb;
+  const unsigned long long k = h == ULLONG_MAX ? ULLONG_MAX : (h << 32);
+  want[i] = k;
+  wrev[s - 1 - i] = k;
 }
 
 constexpr int kSelThreads = 1024;
@@ -295,7 +391,8 @@ __global__ void __launch_bounds__(kSelThreads) k_seed_select(DevSeries S,
       const int i = (int)(wn & 0xffffffffu);
       seeds[round] = make_int2(i < pj ? i : pj, i < pj ? pj : i);
       if (round == 0) {
-        const unsigned long long bits = ((wn >> 32) + 1ull) << 32;
+        // rounded up past the 3 cleared low bits of the key: ED^2 >= DTW^2
+        const unsigned long long bits = (((wn >> 32) & ~7ull) + 8ull) << 32;
         const float e2 = __double2float_ru(__longlong_as_double((long long)bits));
         bsf2[b] = __float_as_uint(e2);
       }
@@ -328,15 +425,45 @@ void launch_mp(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long 
                cudaStream_t st, unsigned int* tile_best) {
   k_fill_u64<<<1024, 256, 0, st>>>(keys, S.s, ULLONG_MAX);
   if (ntiles <= 0) return;
-  static OncePerDevice setup;
-  setup.run([] {
-    cudaFuncSetAttribute(k_mp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MpShared));
-  });
+  cudaFuncSetAttribute(k_mp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(MpShared));
   const int slab = 1 << 20;
   for (int b = 0; b < ntiles; b += slab) {
     const int cnt = ntiles - b < slab ? ntiles - b : slab;
-    k_mp<<<cnt, kLbThreads, sizeof(MpShared), st>>>(S, tiles + b, keys, tile_best, b);
+    k_mp<false><<<cnt, kLbThreads, sizeof(MpShared), st>>>(S, tiles + b, keys, tile_best, b,
+                                                           MpCollect{});
   }
+}
+
+void launch_mp_collect(const DevSeries& S, const Tile* tiles, int ntiles,
+                       const unsigned long long* want, int2* cand, unsigned int* count,
+                       unsigned int cap, cudaStream_t st) {
+  if (ntiles <= 0) return;
+  cudaFuncSetAttribute(k_mp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(MpShared));
+  const int slab = 1 << 20;
+  for (int b = 0; b < ntiles; b += slab) {
+    const int cnt = ntiles - b < slab ? ntiles - b : slab;
+    k_mp<true><<<cnt, kLbThreads, sizeof(MpShared), st>>>(S, tiles + b, nullptr, nullptr, b,
+                                                          MpCollect{want, cand, count, cap});
+  }
+}
+
+void launch_mp_want(int64_t s, const unsigned long long* up, const unsigned long long* lo,
+                    unsigned long long* want, unsigned long long* wrev, cudaStream_t st) {
+  k_mp_want<<<(unsigned)((s + 255) / 256), 256, 0, st>>>(s, up, lo, want, wrev);
+}
+
+void launch_mp_exact(const DevSeries& S, const int2* cand, const unsigned int* count,
+                     unsigned int cap, bool reversed, bool pick, unsigned long long* rowmin,
+                     unsigned long long* rowidx, cudaStream_t st) {
+  k_mp_exact<<<148 * 8, 256, 0, st>>>(S, cand, count, cap, reversed, pick, rowmin, rowidx);
+}
+
+void launch_mp_exact_out(int64_t s, const unsigned long long* rowmin,
+                         const unsigned long long* rowidx, double* mp, int64_t* mpi,
+                         cudaStream_t st) {
+  k_mp_exact_out<<<(unsigned)((s + 255) / 256), 256, 0, st>>>(s, rowmin, rowidx, mp, mpi);
 }
 
 void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,

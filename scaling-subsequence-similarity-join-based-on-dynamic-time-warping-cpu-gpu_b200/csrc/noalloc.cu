@@ -12,7 +12,6 @@
 
 #include <climits>
 #include <cstring>
-#include <mutex>
 
 namespace dtwj {
 void launch_stats(const DevSeries& S, cudaStream_t st);
@@ -31,24 +30,17 @@ constexpr size_t kScratchBytes = (size_t)kMaxWindows * 25;
 
 static __device__ __align__(256) unsigned char g_pair_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
-
-// Device address of the scratch on the current device, looked up once per
-// device (the host-side name of the array is not a device address).
-int scratch_address(int device, void** out) {
-  if (device < 0 || device >= kMaxDevices) return DTWJ_ERR_NODEVICE;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_pair_scratch) != cudaSuccess || !p) {
-      cudaGetLastError();
-      return DTWJ_ERR_CUDA;
-    }
-    g_scratch_addr[device] = p;
+// Device address of the scratch on the current device.  The host-side name
+// of the array is only a stand-in, so the address is looked up on every call
+// with the caller's device current: the lookup allocates nothing, and it stays
+// right after cudaDeviceReset, when the module may come back elsewhere.
+int scratch_address(void** out) {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_pair_scratch) != cudaSuccess || !p) {
+    cudaGetLastError();
+    return DTWJ_ERR_CUDA;
   }
-  *out = g_scratch_addr[device];
+  *out = p;
   return DTWJ_OK;
 }
 
@@ -58,7 +50,8 @@ extern "C" int dtwj_pair_dtw_noalloc(const double* x_dev, int64_t n, int32_t m, 
                                      const int64_t* pi_dev, const int64_t* pj_dev, int64_t count,
                                      int32_t precise, double* dist_dev, void* stream) {
   if (!x_dev || count < 0 || (count > 0 && (!pi_dev || !pj_dev || !dist_dev))) return DTWJ_ERR_ARG;
-  if (m < 8 || w < 0 || n < 2 * (int64_t)m + 1 || n > (int64_t)INT32_MAX - 4) return DTWJ_ERR_ARG;
+  if (m < 8 || m > DTWJ_MAX_M || w < 0 || n < 2 * (int64_t)m + 1 || n > (int64_t)INT32_MAX - 4)
+    return DTWJ_ERR_ARG;
   const int64_t s = n - m + 1;
   if (s > kMaxWindows) return DTWJ_ERR_SCRATCH;
   if (count == 0) return DTWJ_OK;
@@ -71,7 +64,7 @@ extern "C" int dtwj_pair_dtw_noalloc(const double* x_dev, int64_t n, int32_t m, 
     return DTWJ_ERR_NODEVICE;
   }
   void* base = nullptr;
-  int rc = scratch_address(device, &base);
+  int rc = scratch_address(&base);
   if (rc) return rc;
   unsigned char* b = static_cast<unsigned char*>(base);
   DevSeries S;

@@ -445,10 +445,7 @@ void run_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
   }
   const int gpb = threads / G;
   bytes = (size_t)gpb * lay.total * sizeof(float);
-  static OncePerDevice setup;
-  setup.run([] {
-    cudaFuncSetAttribute(k_pairs<C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  });
+  cudaFuncSetAttribute(k_pairs<C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs<C, G>, threads, bytes);
   if (per_sm < 1) per_sm = 1;
@@ -468,11 +465,8 @@ void run_list(const DevSeries& S, const int2* pairs, const Candidate* cands,
     bytes /= 2;
   }
   bytes = (size_t)(threads / G) * elems * sizeof(T);
-  static OncePerDevice setup;
-  setup.run([] {
-    cudaFuncSetAttribute(k_dtw_list<T, C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-  });
+  cudaFuncSetAttribute(k_dtw_list<T, C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       200 * 1024);
   const int groups = threads / G;
   int blocks = (count + groups - 1) / groups;
   if (blocks < 1) blocks = 1;
@@ -650,11 +644,8 @@ void run_pairs64(const DevSeries& S, const int64_t* pi, const int64_t* pj, int64
     bytes /= 2;
   }
   bytes = (size_t)(threads / G) * elems * sizeof(T);
-  static OncePerDevice setup;
-  setup.run([] {
-    cudaFuncSetAttribute(k_dtw_pairs64<T, C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         200 * 1024);
-  });
+  cudaFuncSetAttribute(k_dtw_pairs64<T, C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       200 * 1024);
   const int groups = threads / G;
   int64_t blocks = (count + groups - 1) / groups;
   if (blocks < 1) blocks = 1;

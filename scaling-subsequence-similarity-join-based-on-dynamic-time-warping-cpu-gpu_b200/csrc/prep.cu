@@ -177,7 +177,9 @@ __global__ void k_zmax(DevSeries S, float* zmax) {
       mn = fmin(mn, x);
     }
     double z = fmax(fabs((mx - S.mu[i]) * S.isg[i]), fabs((mn - S.mu[i]) * S.isg[i]));
-    v = (float)z;
+    // rounded down: the table length takes floor(max |z|), which a value just
+    // below an integer must not reach by rounding up
+    v = __double2float_rd(z);
   }
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) atomicMax((unsigned int*)zmax, __float_as_uint(v));

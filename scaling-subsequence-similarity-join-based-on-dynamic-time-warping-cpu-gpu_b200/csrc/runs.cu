@@ -225,7 +225,8 @@ __global__ void __launch_bounds__(kRunWarps * 32, 8) k_runs(DevSeries S, DevSear
     if (lane == 0) item = atomicAdd(Q.run_next, 1u);
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= total_items) break;
-    const unsigned int* src = bits + (size_t)item * kLbWords;
+    // the lag's words, [tile][word][lag]
+    const unsigned int* src = bits + (size_t)(item / kLbLags) * kLbLags * kLbWords + item % kLbLags;
     const Tile T = tiles[item / kLbLags];
     const int64_t L = (int64_t)T.L0 + (int64_t)(item % kLbLags);
     // rows this lag really has in the tile: r < rows and i0 + r + L < s
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(kRunWarps * 32, 8) k_runs(DevSeries S, DevSear
     if (nrow > T.rows) nrow = T.rows;
     bool nz = false;
     for (int x = lane; x < kLbWords; x += 32) {
-      unsigned int v = src[x];
+      unsigned int v = src[(size_t)x * kLbLags];
       const int64_t lo_row = (int64_t)x * 32;
       if (lo_row >= nrow) v = 0u;
       else if (lo_row + 32 > nrow) v &= (1u << (nrow - lo_row)) - 1u;
@@ -373,6 +374,7 @@ __global__ void __launch_bounds__(kKeoghWarps * 32, 5) k_keogh(DevSeries S, DevS
   __shared__ KeoghSide side[kKeoghWarps][kKeoghBatch][2];
   __shared__ float endsv[kKeoghWarps][kKeoghBatch][2];
   __shared__ int serv[kKeoghWarps][kKeoghBatch];
+  __shared__ float errv[kKeoghWarps][kKeoghBatch];  // FP32 error scale of the pair
   __shared__ unsigned long long pruned_block;
   if (threadIdx.x == 0) pruned_block = 0;
   __syncthreads();
@@ -412,11 +414,16 @@ __global__ void __launch_bounds__(kKeoghWarps * 32, 5) k_keogh(DevSeries S, DevS
         t = fma(dd, dd, t);
       }
       endsv[warp][e][d] = (float)fmax((double)__int_as_float(r.z), t);
-      if (d == 0) serv[warp][e] = r.w;
+      if (d == 0) {
+        serv[warp][e] = r.w;
+        errv[warp][e] = fmaxf(S.rw[r.x], S.rw[r.y]);
+      }
     }
     __syncwarp();
     for (int e = 0; e < cnt; ++e) {
-      const float thr = prune_threshold_now(Q.bsf2 + serv[warp][e], S.m);
+      float thr = prune_threshold_now(Q.bsf2 + serv[warp][e], S.m);
+      // a pair whose FP32 error bound does not fit the slack is never pruned here
+      if (!fp32_bound_ok(errv[warp][e], thr, S.m)) thr = __int_as_float(0x7f800000);
       const KeoghSide& wi = side[warp][e][0];
       const KeoghSide& wj = side[warp][e][1];
       bool live = keogh_within(S, wi, wj, endsv[warp][e][0], thr, lane);

@@ -39,8 +39,9 @@ def tiles(n, m):
 
 def upper_profile(x, m, mu, isg):
     """keys of the profile pass: for each row i, the smallest ED^2 over
-    j >= i + m truncated to its high 32 bits, and the partner (lowest j on
-    ties); (inf, -1) without a partner."""
+    j >= i + m truncated to its high 32 bits with the 3 lowest of them
+    cleared, and the partner (lowest j on ties); (inf, -1) without a
+    partner."""
     s = x.size - m + 1
     W = np.lib.stride_tricks.sliding_window_view(x, m)[:s]
     Z = (W - mu[:, None]) * isg[:, None]
@@ -51,7 +52,7 @@ def upper_profile(x, m, mu, isg):
         k = int(np.argmin(e))
         d2[i] = e[k]
         part[i] = i + m + k
-    bits = d2.view(np.uint64) & np.uint64(0xFFFFFFFF00000000)
+    bits = d2.view(np.uint64) & np.uint64(0xFFFFFFF800000000)
     trunc = np.where(np.isfinite(d2), bits.view(np.float64), np.inf)
     return trunc, part
 

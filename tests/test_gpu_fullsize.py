@@ -1,35 +1,55 @@
-"""Full-size checks (the 1M-sample bench workload and the 262k random walk)
-through properties that need no CPU oracle run (an FP64 oracle join at 1M
-samples takes hours): the reported distance is the FP64 DTW of the reported
-pair, no smaller DTW exists at the planted motif pair, and every flag, shard
-count and order that must not change the result reproduces it exactly."""
-import numpy as np
+"""Full-size joins against the oracle: the bench workload (n = 1,000,000,
+m = 1024, w = 52) and the band/shape sweep at 262,144 samples, checked
+against the oracle's top-1 pair on the same seeded series
+(tests/golden/fullsize.json, made by tests/golden/make_fullsize.py with the
+OpenMP FP64 restatement that tests/test_oracle.py pins to the reference).
+Tolerances: indices bit-exact, distance within 1e-5 relative.  Beside the
+oracle, properties every full-size join must have: the distance is the FP64
+DTW of the reported pair, no planted motif pair beats it, and every flag,
+run filter and shard count that must not change the result reproduces it."""
+import json
+import os
+
 import pytest
+
+from conftest import GOLDEN
 
 pytestmark = pytest.mark.gpu
 
+REL = 1e-5
 
-@pytest.mark.parametrize("name", ["rw1m_motif", "rw262k_w52"])
-def test_full_size_join_properties(gpu_dtwj, synth, name):
-    wl = synth.workload(name)
+
+def _records():
+    path = os.path.join(GOLDEN, "fullsize.json")
+    if not os.path.exists(path):
+        return []
+    with open(path) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("rec", _records(), ids=lambda r: r["workload"])
+def test_full_size_join_matches_oracle(gpu_dtwj, synth, rec):
+    wl = synth.workload(rec["workload"])
     x, m, w = wl["series"], wl["m"], wl["w"]
+    assert (x.size, m, w) == (rec["n"], rec["m"], rec["w"])
     with gpu_dtwj.Context() as ctx:
         r = ctx.join(x, m, w)
-        assert r.j - r.i >= m
+        assert (r.i, r.j) == (rec["i"], rec["j"])
+        assert abs(r.dist - rec["dist"]) <= REL * rec["dist"], (r.dist, rec["dist"])
         s = x.size - m + 1
         assert r.pairs == (s - m) * (s - m + 1) // 2
         # the distance is the exact FP64 DTW of the pair
         d = gpu_dtwj.pair_dtw(x, m, w, [r.i], [r.j], precise=True)[0]
         assert r.dist == pytest.approx(d, rel=1e-12)
-        # the ED seeds bound it from above; a planted motif pair cannot beat it
         assert r.dist <= r.seed_bsf * (1 + 1e-6)
         for a, b in wl.get("planted", []):
             dp = gpu_dtwj.pair_dtw(x, m, w, [min(a, b)], [max(a, b)], precise=True)[0]
             assert r.dist <= dp * (1 + 1e-12)
+        # the reference's masked cascade, direct launches and two tile shards
         # (F_NO_SEED is for small inputs: with no initial best-so-far the first
         # chunk of a 1M-sample join overflows its queues and is re-swept in
         # one-tile chunks)
-        for fl in (gpu_dtwj.F_NO_MASKED, gpu_dtwj.F_NO_GRAPH):
+        for fl in (gpu_dtwj.F_MASKED_CASCADE, gpu_dtwj.F_NO_GRAPH):
             q = ctx.join(x, m, w, fl)
             assert (q.i, q.j, q.dist) == (r.i, r.j, r.dist), fl
         parts = []

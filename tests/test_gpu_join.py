@@ -53,6 +53,27 @@ def test_flags_do_not_change_the_result(gpu_dtwj, golden):
     assert nd.pruned_fast == 0 and nd.pairs == base.pairs
 
 
+def test_masked_cascade_matches_block_mean_filter(gpu_dtwj, golden):
+    # the run filter's two forms (the default block-mean LB_Keogh bound, and
+    # the reference's masked diagonal bound + endpoint bound) prune different
+    # pairs but return the same top-1; the block-mean bound lets fewer pairs
+    # reach LB_Keogh
+    for c in golden:
+        base = gpu_dtwj.join(c["series"], c["m"], c["w"])
+        casc = gpu_dtwj.join(c["series"], c["m"], c["w"], gpu_dtwj.F_MASKED_CASCADE)
+        kim = gpu_dtwj.join(c["series"], c["m"], c["w"],
+                            gpu_dtwj.F_MASKED_CASCADE | gpu_dtwj.F_NO_MASKED)
+        for r in (casc, kim):
+            assert (r.i, r.j, r.dist) == (base.i, base.j, base.dist), c["name"]
+            assert r.pruned_paa == 0 and r.pruned_fast == base.pruned_fast
+        assert base.pruned_masked == 0 and kim.pruned_masked == 0
+        if c["name"] == "rw20k":
+            assert base.pruned_paa > 0 and casc.pruned_masked > 0
+            reach_base = base.pruned_keogh + base.dtw_calls
+            reach_casc = casc.pruned_keogh + casc.dtw_calls
+            assert reach_base < reach_casc, (reach_base, reach_casc)
+
+
 def test_graph_replay_matches_direct_launches(gpu_dtwj, golden):
     # a context captures the sweep as a CUDA graph on the first join and
     # replays it on the next join of the same shape
@@ -92,13 +113,33 @@ def test_pair_dtw_matches_oracle(gpu_dtwj, oracle, synth):
         np.testing.assert_allclose(d32, ref, rtol=2e-4)
 
 
-def test_matrix_profile_matches_oracle(gpu_dtwj, oracle, synth):
-    x = synth.random_walk(5000, 41)
-    m = 64
+@pytest.mark.parametrize("n,m,seed,kind", [(5000, 64, 41, "rw"), (8000, 128, 42, "rw"),
+                                           (6000, 100, 43, "ecg"), (3000, 16, 44, "rw")])
+def test_matrix_profile_matches_oracle(gpu_dtwj, oracle, synth, n, m, seed, kind):
+    # every row's nearest-neighbour index equals the oracle's (the device keeps
+    # every partner near the row minimum and decides among them at FP64);
+    # distances within 1e-6 (the oracle's 1 - correlation form cancels for
+    # close neighbours)
+    x = synth.random_walk(n, seed) if kind == "rw" else synth.ecg_like(n, seed)
     mp, mpi = gpu_dtwj.matrix_profile(x, m)
     omp, ompi = oracle.mp(x, m)
     np.testing.assert_allclose(mp, omp, rtol=1e-6, atol=1e-6)
-    assert np.mean(mpi == ompi) > 0.999
+    assert np.array_equal(mpi, ompi), np.flatnonzero(mpi != ompi)[:10]
+
+
+def test_global_mask_matches_reference(gpu_dtwj, oracle, synth, kat):
+    # the device's global CDF mask against the reference's own
+    # compute_MASK_global (known answers) and the oracle's restatement
+    for c in kat["mask"]:
+        x = synth.random_walk(c["n"], c["seed"]) if c["kind"] == "rw" else \
+            synth.ecg_like(c["n"], c["seed"])
+        mask, lt = gpu_dtwj.global_mask(x, c["m"], c["w"])
+        assert lt == c["table_len"]
+        ones = np.flatnonzero(mask == 1.0)
+        ref = np.array(c["ones"])
+        assert np.setdiff1d(ones, ref).size + np.setdiff1d(ref, ones).size == 0, c
+        omask, _ = oracle.mask(x, c["m"], c["w"])
+        assert np.array_equal(mask.astype(np.float64), omask)
 
 
 def test_nan_input_is_rejected(gpu_dtwj, synth):
@@ -241,6 +282,45 @@ def test_sharded_join_equals_the_whole(gpu_dtwj, golden, world):
         merged = gpu_dtwj.merge_results(parts)
         _check(merged, c["i"], c["j"], c["dist"], (c["name"], world))
         assert merged.pairs == whole.pairs
+
+
+def test_exchanged_best_so_far_feeds_every_shard(gpu_dtwj, golden):
+    # the best-so-far exchange between shards (dtwj_ctx_set_exchange): here the
+    # callback lowers each shard's best-so-far to the whole join's distance
+    # (squared, rounded up to float: the distance of a real pair), as an
+    # all-reduce over shards would once the shard holding that pair found it.
+    # The shards still merge into the whole join, and they evaluate no more
+    # DTWs than without the exchange.
+    import torch
+
+    c = [g for g in golden if g["name"] == "rw20k"][0]
+    x, m, w = c["series"], c["m"], c["w"]
+    whole = gpu_dtwj.join(x, m, w)
+    cap = int(np.float32(whole.dist ** 2 * (1 + 1e-6)).view(np.int32))
+    calls = []
+
+    def lower(user, ptr, count, stream):
+        words = torch.as_tensor(gpu_dtwj._DeviceWords(ptr, count), device="cuda")
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+            words.clamp_(max=cap)
+        calls.append(count)
+
+    plain, fed = [], []
+    with gpu_dtwj.Context() as ctx:
+        for r in range(2):
+            ctx.set_shard(r, 2)
+            plain.append(ctx.join(x, m, w))
+        ctx.set_exchange(lower, phases=4)
+        for r in range(2):
+            ctx.set_shard(r, 2)
+            fed.append(ctx.join(x, m, w))
+        ctx.set_exchange(None)
+    assert calls == [1] * 8
+    for parts in (plain, fed):
+        merged = gpu_dtwj.merge_results(parts)
+        _check(merged, c["i"], c["j"], c["dist"], "exchange")
+        assert merged.pairs == whole.pairs
+    assert sum(p.dtw_calls for p in fed) <= sum(p.dtw_calls for p in plain)
 
 
 def test_cli_reads_the_reference_file_formats(tmp_path, golden):
