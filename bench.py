@@ -359,16 +359,25 @@ def run_ours(args):
     # the plain-vs-learned comparison the metric names; top-1 must not change
     learned = None
     model_path = os.path.join(os.path.dirname(dtwj.LIB_PATH), "..", "tile_mlp_rw_m256.bin")
-    if os.path.exists(model_path) and not args.no_learned:
+    if os.path.exists(model_path) and not args.no_learned and args.learned_reps > 0:
         net = dtwj.MLP.load_file(os.path.abspath(model_path), device=local)
         ctx.set_model(net)
-        rl = [ctx.join_device(dptr, n, m, w, flags | dtwj.F_LEARNED) for _ in range(2)][-1]
-        learned = {"join_seconds": rl.seconds_join, "plain_join_seconds": r0.seconds_join,
-                   "dtw_calls": rl.dtw_calls, "plain_dtw_calls": r0.dtw_calls,
-                   "identical_top1": (rl.i, rl.j, rl.dist) == (r0.i, r0.j, r0.dist)
+        runs = {"plain": [], "learned": []}
+        for _ in range(args.learned_reps):  # alternating, so drift hits both alike
+            for name, fl in (("plain", flags), ("learned", flags | dtwj.F_LEARNED)):
+                runs[name].append(ctx.join_device(dptr, n, m, w, fl))
+        ctx.set_model(None)
+
+        def stats(rs):
+            t = [r.seconds_join for r in rs]
+            return {"mean": statistics.mean(t), "sd": statistics.stdev(t) if len(t) > 1 else 0.0,
+                    "dtw_calls": rs[-1].dtw_calls, "dtw_cells": rs[-1].dtw_cells}
+        sp, sl = stats(runs["plain"]), stats(runs["learned"])
+        learned = {"reps": args.learned_reps, "plain_join_seconds": sp, "learned_join_seconds": sl,
+                   "gain": 1.0 - sl["mean"] / sp["mean"],
+                   "identical_top1": len({(r.i, r.j, r.dist) for v in runs.values() for r in v}) == 1
                    if world == 1 else None,
                    "model": "tile_mlp_rw_m256.bin (trained on m=256 random walks)"}
-        ctx.set_model(None)
 
     # e2e through the host-pointer API (pinned host buffer)
     fn = dtwj.load().dtwj_ctx_join
@@ -497,6 +506,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=16384)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--learned-reps", type=int, default=5)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

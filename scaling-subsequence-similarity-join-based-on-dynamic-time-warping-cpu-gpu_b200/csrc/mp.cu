@@ -45,7 +45,7 @@ struct MpShared {
   double p1[kCols], p2[kCols], is[kCols], c2[kCols];
   double r1[kStage], r2[kStage], ci[kStage];
   unsigned int lim[kStage];
-  unsigned long long rowbest[kLbRows];
+  unsigned long long rowbest[kStage];  // row minima of the current stage
 };
 
 // Candidate list of the exact profile (COLLECT): every pair whose high word
@@ -58,7 +58,7 @@ struct MpCollect {
 };
 
 template <bool COLLECT>
-__global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* tiles,
+__global__ void __launch_bounds__(kLbThreads, 4) k_mp(DevSeries S, const Tile* tiles,
                                                       unsigned long long* keys,
                                                       unsigned int* tile_best, int tile_base,
                                                       MpCollect col) {
@@ -70,7 +70,6 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
   const int t = threadIdx.x, lane = t & 31;
   const int64_t L0 = T.L0, i0 = T.i0;
   const int64_t Lt = L0 + (int64_t)t * kLbPerThread;
-  for (int x = t; x < T.rows; x += kLbThreads) sh.rowbest[x] = ULLONG_MAX;
 
   // exact anchors C(i0, i0 + L) for the thread's lags
   double C[kLbPerThread];
@@ -96,9 +95,12 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
   }
   double w1[kLbPerThread], w2[kLbPerThread], wi[kLbPerThread], wc[kLbPerThread];
   const double two_m = 2.0 * m;
+  unsigned int tmin = 0xffffffffu;  // the tile's smallest key (high bits of ED^2)
   for (int st = 0; st < T.rows; st += kStage) {
     const int64_t r0 = i0 + st, c0 = r0 + L0;
     __syncthreads();
+    if (!COLLECT)
+      for (int x = t; x < kStage; x += kLbThreads) sh.rowbest[x] = ULLONG_MAX;
     for (int x = t; x < kCols; x += kLbThreads) {
       const int64_t j = c0 + x;
       const bool in = j >= 0 && j < s, up = j >= 1 && j < s;  // update terms exist for j >= 1
@@ -175,23 +177,26 @@ __global__ void __launch_bounds__(kLbThreads, 2) k_mp(DevSeries S, const Tile* t
               const unsigned long long key =
                   ((unsigned long long)(wbest & ~7u) << 32) |
                   (unsigned long long)(unsigned int)(i + Lt + (wbest & 7u));
-              atomicMin(&sh.rowbest[st + r], key);
+              atomicMin(&sh.rowbest[r], key);
             }
           }
         }
       }
     }
-  }
-  if (COLLECT) return;
-  __syncthreads();
-  unsigned int tmin = 0xffffffffu;  // the tile's smallest key (high bits of ED^2)
-  for (int x = t; x < T.rows; x += kLbThreads) {
-    const unsigned long long v = sh.rowbest[x];
-    if (v != ULLONG_MAX) {
-      atomicMin(&keys[i0 + x], v);
-      tmin = min(tmin, (unsigned int)(v >> 32));
+    if (!COLLECT) {
+      // the stage's row minima into the series' keys (each row once per tile)
+      __syncthreads();
+      const int nrow = T.rows - st < kStage ? T.rows - st : kStage;
+      for (int x = t; x < nrow; x += kLbThreads) {
+        const unsigned long long v = sh.rowbest[x];
+        if (v != ULLONG_MAX) {
+          atomicMin(&keys[r0 + x], v);
+          tmin = min(tmin, (unsigned int)(v >> 32));
+        }
+      }
     }
   }
+  if (COLLECT) return;
   if (tile_best) {
     for (int o = 16; o > 0; o >>= 1) tmin = min(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
     if (lane == 0 && tmin != 0xffffffffu) atomicMin(&tile_best[tile_base + blockIdx.x], tmin);

@@ -22,6 +22,9 @@
 // warp.  Survivors on a lag cluster: a nonzero word holds about 28 of 32 rows.
 // The lanes run the block terms of both directions together and vote every
 // four blocks; the batch stops as soon as every live lane is pruned.  The
+// blocks run in warp-wide segments between the points where some lane's
+// window crosses into the next 1024-sample block (its offset changes there),
+// so the loop body is loads at immediate offsets and the block terms only.  The
 // endpoint bound (LB_Kim, CPU_version1/lb_kim.cpp:10-73) then runs in FP64 on
 // the survivors, which go to the LB_Keogh queue.
 //
@@ -140,48 +143,45 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 4) k_paa(DevSeries S, DevSearc
     if (!nz) continue;
     const Tile T = tiles[tk];
     const unsigned int* bsf2 = Q.bsf2 + T.series;
-    const int64_t i = (int64_t)T.i0 + wi * 32 + lane;  // this lane's row
+    const int64_t i_row = (int64_t)T.i0 + wi * 32 + lane;  // this lane's row
     while (nz) {
       const int l = __ffs(nz) - 1;
       nz &= nz - 1u;
       const unsigned int wb = __shfl_sync(0xffffffffu, word, l);
-      const int64_t j = i + (int64_t)T.L0 + g * 32 + l;
       const bool live = (wb >> lane) & 1u;  // the sweep set only bits of valid pairs
+      // a lane without a pair computes the first live lane's pair (valid
+      // addresses, result ignored), so the block loop needs no predicate
+      const int64_t i_src = __shfl_sync(0xffffffffu, i_row, __ffs(wb) - 1);
+      const int64_t i = live ? i_row : i_src;
+      const int64_t j = i + (int64_t)T.L0 + g * 32 + l;
       const float thr = prune_threshold_now(bsf2, m);
+      const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
       // a pair whose FP32 error bound does not fit the slack is never pruned here
-      float thr_lane = __int_as_float(0x7f800000);
-      double mi = 0.0, si = 0.0, mj = 0.0, sj = 0.0;
-      if (live) {
-        mi = S.mu[i];
-        si = S.isg[i];
-        mj = S.mu[j];
-        sj = S.isg[j];
-        if (fp32_bound_ok(fmaxf(S.rw[i], S.rw[j]), thr, m)) thr_lane = thr;
-      }
+      const float thr_lane =
+          live && fp32_bound_ok(fmaxf(S.rw[i], S.rw[j]), thr, m) ? thr : __int_as_float(0x7f800000);
       const float fsi = (float)si, fsj = (float)sj;
-      int64_t xi = i, xj = j;
-      int64_t nexti = 0, nextj = 0;  // first sample of the next 1024-block
-      double oi = 0.0, oj = 0.0;
-      float oij = 0.0f;
+      const float* pai = S.pa + i;
+      const float* paj = S.pa + j;
+      const float2* pui = S.pul + i;
+      const float2* puj = S.pul + j;
+      // the block offsets change where a window's block start crosses a
+      // 1024-sample boundary: block ci (i) and cj (j), then every 1024 / B
+      int ci = (int)((((i >> kBlkShift) + 1) << kBlkShift) - i + B - 1) / B;
+      int cj = (int)((((j >> kBlkShift) + 1) << kBlkShift) - j + B - 1) / B;
+      float oij = (float)(win_offset(S, i >> kBlkShift, mi, si) - win_offset(S, j >> kBlkShift, mj, sj));
       float acc1 = 0.0f, acc2 = 0.0f;
       bool pruned = !live;
-      for (int k = 0; k < nb; k += 4) {
+      int k = 0;
+      while (k < nb) {
+        // a segment of blocks in which no lane's offsets change
+        int seg = min(ci, cj);
+        seg = __reduce_min_sync(0xffffffffu, (unsigned int)min(seg, nb));
+        for (; k + 4 <= seg; k += 4) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          if (k + u < nb && !pruned) {
-            if (xi >= nexti || xj >= nextj) {
-              if (xi >= nexti) {
-                oi = win_offset(S, xi >> kBlkShift, mi, si);
-                nexti = ((xi >> kBlkShift) + 1) << kBlkShift;
-              }
-              if (xj >= nextj) {
-                oj = win_offset(S, xj >> kBlkShift, mj, sj);
-                nextj = ((xj >> kBlkShift) + 1) << kBlkShift;
-              }
-              oij = (float)(oi - oj);
-            }
-            const float ai = S.pa[xi], aj = S.pa[xj];
-            const float2 ui = S.pul[xi], uj = S.pul[xj];
+          for (int u = 0; u < 4; ++u) {
+            const int x = (k + u) * B;
+            const float ai = pai[x], aj = paj[x];
+            const float2 ui = pui[x], uj = puj[x];
             // query i against the envelope of j: q - U = P - Uj sj, L - q = Lj sj - P
             const float p1 = fmaf(ai, fsi, oij);
             const float d1 = max3f(fmaf(-uj.x, fsj, p1), fmaf(uj.y, fsj, -p1), 0.0f);
@@ -190,13 +190,33 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 4) k_paa(DevSeries S, DevSearc
             const float p2 = fmaf(aj, fsj, -oij);
             const float d2 = max3f(fmaf(-ui.x, fsi, p2), fmaf(ui.y, fsi, -p2), 0.0f);
             acc2 = fmaf(d2, d2, acc2);
-            xi += B;
-            xj += B;
           }
+          pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
+          if (__all_sync(0xffffffffu, pruned)) break;
         }
-        pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
         if (__all_sync(0xffffffffu, pruned)) break;
+        for (; k < seg; ++k) {
+          const int x = k * B;
+          const float ai = pai[x], aj = paj[x];
+          const float2 ui = pui[x], uj = puj[x];
+          const float p1 = fmaf(ai, fsi, oij);
+          const float d1 = max3f(fmaf(-uj.x, fsj, p1), fmaf(uj.y, fsj, -p1), 0.0f);
+          acc1 = fmaf(d1, d1, acc1);
+          const float p2 = fmaf(aj, fsj, -oij);
+          const float d2 = max3f(fmaf(-ui.x, fsi, p2), fmaf(ui.y, fsi, -p2), 0.0f);
+          acc2 = fmaf(d2, d2, acc2);
+        }
+        if (k >= nb) break;
+        // at block k some lanes cross into the next 1024-sample block
+        if (k == ci || k == cj) {
+          if (k == ci) ci += (1 << kBlkShift) / B;
+          if (k == cj) cj += (1 << kBlkShift) / B;
+          const int64_t xi = i + (int64_t)k * B, xj = j + (int64_t)k * B;
+          oij = (float)(win_offset(S, xi >> kBlkShift, mi, si) -
+                        win_offset(S, xj >> kBlkShift, mj, sj));
+        }
       }
+      pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
       bool alive = live && !pruned;
       npaa += (live && pruned) ? 1u : 0u;
       float kim = 0.0f;
