@@ -141,8 +141,7 @@ struct DevSeries {
   float* af;        // n, a - cb[block]
   float2* ulf;      // n, (U - cb[block], L - cb[block])
   int paa_b;        // block length of the block-mean bound (8, 16 or 32)
-  float* pa;        // n, mean of a[p, p + paa_b) - cb[block of p]
-  float2* pul;      // n, the same means of (U, L)
+  float4* pq;       // n, means over [p, p + paa_b) of (a, U, L) - cb[block of p], 0
   float* cmax;      // (n >> kBlkShift) + 2, largest |centered FP32 value| per block
   float* rw;        // s, FP32 error scale of window i: isg_i x the largest
                     //    centered magnitude or block offset its FP32 bounds read
@@ -284,7 +283,7 @@ void launch_paa(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int t
                 int tile_end, const unsigned int* bits, int num_sms, cudaStream_t st);
 // Block length of the block-mean bound for windows of length m.
 int paa_block(int m);
-// Sliding block means (pa, pul), per-block magnitudes (cmax) and per-window
+// Sliding block means (pq), per-block magnitudes (cmax) and per-window
 // error scales (rw); after launch_center.
 void launch_paa_prep(const DevSeries& S, cudaStream_t st);
 // LB_Keogh over the candidates the run filter queued in Q.kq; survivors go to

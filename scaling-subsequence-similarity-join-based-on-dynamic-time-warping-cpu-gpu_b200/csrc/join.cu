@@ -81,7 +81,7 @@ enum BufId {
   B_COUNTS, B_DIFF, B_MEAN, B_ZMAX, B_KEYS_UP, B_QUEUE, B_QCOUNT,
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
   B_MP, B_MPI, B_CB, B_AF, B_ULF, B_BITS, B_LBTILES, B_KQ, B_SBEG, B_SID, B_SEEDBSF,
-  B_BEST_IJ, B_BEST_F32, B_QSER, B_TILEBEST, B_FEAT, B_SCORE, B_PA, B_PUL, B_CMAX, B_RW,
+  B_BEST_IJ, B_BEST_F32, B_QSER, B_TILEBEST, B_FEAT, B_SCORE, B_PA, B_CMAX, B_RW,
   B_MPX_WANT, B_MPX_WREV, B_MPX_MIN, B_MPX_IDX, B_MPX_CAND, B_MPX_CNT,
   B_COUNT_
 };
@@ -258,8 +258,7 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   ENSURE(B_CB, ((n >> kBlkShift) + 4) * 8, S.cb);
   ENSURE(B_AF, n * 4, S.af);
   ENSURE(B_ULF, n * 8, S.ulf);
-  ENSURE(B_PA, n * 4, S.pa);
-  ENSURE(B_PUL, n * 8, S.pul);
+  ENSURE(B_PA, n * 16, S.pq);
   ENSURE(B_CMAX, ((n >> kBlkShift) + 4) * 4, S.cmax);
   ENSURE(B_RW, s * 4, S.rw);
   S.paa_b = paa_block(m);

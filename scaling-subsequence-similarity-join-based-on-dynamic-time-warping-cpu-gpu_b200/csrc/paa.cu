@@ -16,15 +16,20 @@
 //
 // Work items are (tile, 32-row word, group of 32 lags) of the diagonal
 // sweep's survivor bits, stored [tile][word][lag].  A warp loads the 32 words
-// of its lag group in one coalesced read; for every lag with survivors, lane p
-// takes row p of the word, so the 32 pairs are consecutive on one diagonal and
-// every block read (pa, pul at i + B k and j + B k) is one contiguous line per
-// warp.  Survivors on a lag cluster: a nonzero word holds about 28 of 32 rows.
-// The lanes run the block terms of both directions together and vote every
+// of its lag group in one coalesced read; for every lag L with survivors,
+// lane p takes row i = i0 + p of the word (survivors cluster: a nonzero word
+// holds about 28 of 32 rows).  The blocks are aligned to absolute sample
+// positions: block [x, x + B) of window i, x a multiple of B, meets block
+// [x + L, x + L + B) of window j, so every lane of the batch reads the same
+// two block means (broadcast loads) and only the per-window normalisation
+// differs between lanes.  The aligned blocks inside every lane's window are
+// shared; each lane adds the window-relative blocks that fit in its own
+// window before and after them (the rows are consecutive, so those reads are
+// coalesced).  A window's block offset changes where a block crosses a
+// 1024-sample boundary; for aligned blocks that happens at the same block in
+// every lane, so the shared blocks run in warp-wide segments with constant
+// offsets: two loads and ten FP32 operations per block.  The lanes vote every
 // four blocks; the batch stops as soon as every live lane is pruned.  The
-// blocks run in warp-wide segments between the points where some lane's
-// window crosses into the next 1024-sample block (its offset changes there),
-// so the loop body is loads at immediate offsets and the block terms only.  The
 // endpoint bound (LB_Kim, CPU_version1/lb_kim.cpp:10-73) then runs in FP64 on
 // the survivors, which go to the LB_Keogh queue.
 //
@@ -47,15 +52,14 @@ __device__ __forceinline__ float max3f(float a, float b, float c) {
 }
 
 // Sliding block means, centered on the 1024-sample block of their first
-// sample: pa[p] = mean a[p, p + B) - cb[p >> kBlkShift], pul likewise for
-// (U, L).  Entries whose block runs past the series are zero (never read:
-// a window's blocks end inside it).
+// sample: pq[p] = (means over [p, p + B) of a, U, L) - cb[p >> kBlkShift].
+// Entries whose block runs past the series are zero (never read: a window's
+// blocks end inside it).
 __global__ void k_slide_means(DevSeries S, int B) {
   const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= S.n) return;
   if (p + B > S.n) {
-    S.pa[p] = 0.0f;
-    S.pul[p] = make_float2(0.0f, 0.0f);
+    S.pq[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     return;
   }
   double sa = 0.0, su = 0.0, sl = 0.0;
@@ -65,12 +69,11 @@ __global__ void k_slide_means(DevSeries S, int B) {
     sl += S.L[p + k];
   }
   const double c = S.cb[p >> kBlkShift], ib = 1.0 / (double)B;
-  S.pa[p] = (float)(sa * ib - c);
-  S.pul[p] = make_float2((float)(su * ib - c), (float)(sl * ib - c));
+  S.pq[p] = make_float4((float)(sa * ib - c), (float)(su * ib - c), (float)(sl * ib - c), 0.0f);
 }
 
 // cmax[b] = the largest magnitude of any centered FP32 value of block b
-// (af, ulf, pa, pul), read by LB_Keogh and the block-mean bound.
+// (af, ulf, pq), read by LB_Keogh and the block-mean bound.
 __global__ void k_block_max(DevSeries S, int nb) {
   const int b = blockIdx.x;
   if (b >= nb) return;
@@ -79,9 +82,10 @@ __global__ void k_block_max(DevSeries S, int nb) {
   if (hi > S.n) hi = S.n;
   float v = 0.0f;
   for (int64_t p = lo + threadIdx.x; p < hi; p += blockDim.x) {
-    const float2 u = S.ulf[p], pu = S.pul[p];
+    const float2 u = S.ulf[p];
+    const float4 q = S.pq[p];
     v = fmaxf(v, fmaxf(fabsf(S.af[p]), fmaxf(fabsf(u.x), fabsf(u.y))));
-    v = fmaxf(v, fmaxf(fabsf(S.pa[p]), fmaxf(fabsf(pu.x), fabsf(pu.y))));
+    v = fmaxf(v, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
   }
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   __shared__ float red[8];
@@ -118,8 +122,21 @@ struct Ends6 {
   __device__ double operator[](int k) const { return v[k]; }
 };
 
+// One block term of both directions: query i (block mean qi) against the
+// envelope of j (uj, lj) and query j against the envelope of i, with
+// q - U = P - U s and L - q = L s - P, P = q s + (offset of q - offset of U).
+__device__ __forceinline__ void block_terms(const float4 bi, const float4 bj, float si, float sj,
+                                            float oij, float& acc1, float& acc2) {
+  const float p1 = fmaf(bi.x, si, oij);
+  const float d1 = max3f(fmaf(-bj.y, sj, p1), fmaf(bj.z, sj, -p1), 0.0f);
+  acc1 = fmaf(d1, d1, acc1);
+  const float p2 = fmaf(bj.x, sj, -oij);
+  const float d2 = max3f(fmaf(-bi.y, si, p2), fmaf(bi.z, si, -p2), 0.0f);
+  acc2 = fmaf(d2, d2, acc2);
+}
+
 template <int B>
-__global__ void __launch_bounds__(kPaaWarps * 32, 4) k_paa(DevSeries S, DevSearch Q,
+__global__ void __launch_bounds__(kPaaWarps * 32, 3) k_paa(DevSeries S, DevSearch Q,
                                                            const Tile* tiles,
                                                            const unsigned int* bits,
                                                            unsigned int total_items) {
@@ -128,7 +145,7 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 4) k_paa(DevSeries S, DevSearc
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const int m = S.m;
-  const int nb = m / B;  // whole blocks; a partial tail block is left out (terms >= 0)
+  constexpr int kSpan = 1 << kBlkShift;
   unsigned int npaa = 0, nkim = 0;
   for (;;) {
     unsigned int item = 0;
@@ -143,80 +160,75 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 4) k_paa(DevSeries S, DevSearc
     if (!nz) continue;
     const Tile T = tiles[tk];
     const unsigned int* bsf2 = Q.bsf2 + T.series;
-    const int64_t i_row = (int64_t)T.i0 + wi * 32 + lane;  // this lane's row
+    const int64_t ib = (int64_t)T.i0 + wi * 32;  // the batch's first row
+    // aligned blocks inside every row's window [ib + p, ib + p + m), p < 32
+    // (none when m is short: each lane then covers its window by itself)
+    int64_t x_lo = (ib + 31 + B - 1) / B * B, x_hi = (ib + m) / B * B;
+    const bool shared = x_lo < x_hi;
+    if (!shared) x_lo = x_hi = 0;
     while (nz) {
       const int l = __ffs(nz) - 1;
       nz &= nz - 1u;
       const unsigned int wb = __shfl_sync(0xffffffffu, word, l);
       const bool live = (wb >> lane) & 1u;  // the sweep set only bits of valid pairs
+      const int64_t L = (int64_t)T.L0 + g * 32 + l;
       // a lane without a pair computes the first live lane's pair (valid
-      // addresses, result ignored), so the block loop needs no predicate
-      const int64_t i_src = __shfl_sync(0xffffffffu, i_row, __ffs(wb) - 1);
-      const int64_t i = live ? i_row : i_src;
-      const int64_t j = i + (int64_t)T.L0 + g * 32 + l;
+      // addresses, result ignored), so the block loops need no predicate
+      const int src = __ffs(wb) - 1;
+      const int64_t i = ib + (live ? lane : src), j = i + L;
       const float thr = prune_threshold_now(bsf2, m);
       const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
       // a pair whose FP32 error bound does not fit the slack is never pruned here
       const float thr_lane =
           live && fp32_bound_ok(fmaxf(S.rw[i], S.rw[j]), thr, m) ? thr : __int_as_float(0x7f800000);
       const float fsi = (float)si, fsj = (float)sj;
-      const float* pai = S.pa + i;
-      const float* paj = S.pa + j;
-      const float2* pui = S.pul + i;
-      const float2* puj = S.pul + j;
-      // the block offsets change where a window's block start crosses a
-      // 1024-sample boundary: block ci (i) and cj (j), then every 1024 / B
-      int ci = (int)((((i >> kBlkShift) + 1) << kBlkShift) - i + B - 1) / B;
-      int cj = (int)((((j >> kBlkShift) + 1) << kBlkShift) - j + B - 1) / B;
-      float oij = (float)(win_offset(S, i >> kBlkShift, mi, si) - win_offset(S, j >> kBlkShift, mj, sj));
       float acc1 = 0.0f, acc2 = 0.0f;
-      bool pruned = !live;
-      int k = 0;
-      while (k < nb) {
-        // a segment of blocks in which no lane's offsets change
-        int seg = min(ci, cj);
-        seg = __reduce_min_sync(0xffffffffu, (unsigned int)min(seg, nb));
-        for (; k + 4 <= seg; k += 4) {
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int x = (k + u) * B;
-            const float ai = pai[x], aj = paj[x];
-            const float2 ui = pui[x], uj = puj[x];
-            // query i against the envelope of j: q - U = P - Uj sj, L - q = Lj sj - P
-            const float p1 = fmaf(ai, fsi, oij);
-            const float d1 = max3f(fmaf(-uj.x, fsj, p1), fmaf(uj.y, fsj, -p1), 0.0f);
-            acc1 = fmaf(d1, d1, acc1);
-            // query j against the envelope of i
-            const float p2 = fmaf(aj, fsj, -oij);
-            const float d2 = max3f(fmaf(-ui.x, fsi, p2), fmaf(ui.y, fsi, -p2), 0.0f);
-            acc2 = fmaf(d2, d2, acc2);
+      // ---- this lane's own blocks before and after the shared ones ----
+      {
+        // head [i, x_lo) and tail [x_hi, i + m) are each at most 30 + B
+        // samples long; without shared blocks the head is the whole window
+        // (m < 31 + 2B, so at most 2 (30 + B) / B blocks as well)
+        const int nh = shared ? (int)((x_lo - i) / B) : m / B;
+        const int nt = shared ? (int)((i + m - x_hi) / B) : 0;
+        constexpr int kEdgeMax = 2 * ((30 + B) / B);
+#pragma unroll 1
+        for (int e = 0; e < kEdgeMax; ++e) {
+          const bool head = e < nh, tail = e >= nh && e < nh + nt;
+          if (head || tail) {
+            const int64_t xi = head ? i + (int64_t)e * B : x_hi + (int64_t)(e - nh) * B;
+            const int64_t xj = xi + L;
+            const float o = (float)(win_offset(S, xi >> kBlkShift, mi, si) -
+                                    win_offset(S, xj >> kBlkShift, mj, sj));
+            block_terms(S.pq[xi], S.pq[xj], fsi, fsj, o, acc1, acc2);
           }
+        }
+      }
+      // ---- the shared aligned blocks, in segments of constant offsets ----
+      bool pruned = !live || (float)B * fmaxf(acc1, acc2) > thr_lane;
+      int64_t x = x_lo;
+      while (x < x_hi && !__all_sync(0xffffffffu, pruned)) {
+        // the next block whose i or j side starts in another 1024-sample block
+        const int64_t ci = (x / kSpan + 1) * kSpan;
+        const int64_t cj = ((((x + L) / kSpan + 1) * kSpan - L) + B - 1) / B * B;
+        int64_t seg = ci < cj ? ci : cj;
+        if (seg > x_hi) seg = x_hi;
+        const float oij = (float)(win_offset(S, x >> kBlkShift, mi, si) -
+                                  win_offset(S, (x + L) >> kBlkShift, mj, sj));
+        const float4* qi = S.pq + x;
+        const float4* qj = S.pq + x + L;
+        const int nblk = (int)((seg - x) / B);
+        int k = 0;
+        for (; k + 4 <= nblk; k += 4, qi += 4 * B, qj += 4 * B) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) block_terms(qi[u * B], qj[u * B], fsi, fsj, oij, acc1, acc2);
           pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
           if (__all_sync(0xffffffffu, pruned)) break;
         }
-        if (__all_sync(0xffffffffu, pruned)) break;
-        for (; k < seg; ++k) {
-          const int x = k * B;
-          const float ai = pai[x], aj = paj[x];
-          const float2 ui = pui[x], uj = puj[x];
-          const float p1 = fmaf(ai, fsi, oij);
-          const float d1 = max3f(fmaf(-uj.x, fsj, p1), fmaf(uj.y, fsj, -p1), 0.0f);
-          acc1 = fmaf(d1, d1, acc1);
-          const float p2 = fmaf(aj, fsj, -oij);
-          const float d2 = max3f(fmaf(-ui.x, fsi, p2), fmaf(ui.y, fsi, -p2), 0.0f);
-          acc2 = fmaf(d2, d2, acc2);
-        }
-        if (k >= nb) break;
-        // at block k some lanes cross into the next 1024-sample block
-        if (k == ci || k == cj) {
-          if (k == ci) ci += (1 << kBlkShift) / B;
-          if (k == cj) cj += (1 << kBlkShift) / B;
-          const int64_t xi = i + (int64_t)k * B, xj = j + (int64_t)k * B;
-          oij = (float)(win_offset(S, xi >> kBlkShift, mi, si) -
-                        win_offset(S, xj >> kBlkShift, mj, sj));
-        }
+        if (k + 4 <= nblk) break;  // every lane pruned
+        for (; k < nblk; ++k, qi += B, qj += B) block_terms(qi[0], qj[0], fsi, fsj, oij, acc1, acc2);
+        pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
+        x = seg;
       }
-      pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
       bool alive = live && !pruned;
       npaa += (live && pruned) ? 1u : 0u;
       float kim = 0.0f;
