@@ -455,7 +455,8 @@ def run_ours(args):
                    "parallelism": "tile shards x%d" % world if world > 1 else "single"},
         "join_seconds": dev_seconds / args.steps,
         "result": {"i": r0.i, "j": r0.j, "dist": r0.dist},
-        "pruned": {"fast": r0.pruned_fast, "masked": r0.pruned_masked, "kim": r0.pruned_kim,
+        "pruned": {"fast": r0.pruned_fast, "paa": r0.pruned_paa, "masked": r0.pruned_masked,
+                   "kim": r0.pruned_kim,
                    "keogh": r0.pruned_keogh, "dtw_calls": r0.dtw_calls,
                    "dtw_abandoned": r0.dtw_abandoned},
         "dtw_cells_per_s": cells_per_s,
