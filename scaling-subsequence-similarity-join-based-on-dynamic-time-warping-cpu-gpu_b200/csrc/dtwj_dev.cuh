@@ -253,8 +253,14 @@ void launch_mp_exact_out(int64_t s, const unsigned long long* rowmin,
 // kSeeds seeds per series into seeds[series * kSeeds ...] (unused slots hold
 // (-1, -1)), their counts into nseeds[series] and the initial best-so-far
 // into bsf2[series].
+// key_bound: also set bsf2 from the best key (an exact FP64 profile only).
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
-                        unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st);
+                        unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st,
+                        bool key_bound);
+// Row minima for the join's seeds: FP64 anchors and stage carries, FP32
+// increments within a stage (keys only rank the seed candidates).
+void launch_mp_seed(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long long* keys,
+                    cudaStream_t st);
 // Series of a sample (0 for a single series).
 __device__ __forceinline__ int series_of(const DevSeries& S, int64_t x) {
   return S.sid ? S.sid[x] : 0;

@@ -433,7 +433,10 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
       CUDA_OK(cudaMemsetAsync(tbest, 0xff, (size_t)nlb * 4, st));
     }
     ph.begin();
-    launch_mp(S, lbtiles, nlb, keys, st, tbest);
+    // a join only ranks seed candidates by these keys (mixed precision); the
+    // per-tile minima and the exported features take the exact FP64 profile
+    if (tq) launch_mp(S, lbtiles, nlb, keys, st, tbest);
+    else launch_mp_seed(S, lbtiles, nlb, keys, st);
     if (tile_mode) launch_tile_bound(tbest, nlb, Q.bsf2, st);
     ph.end(DTWJ_PHASE_PROFILE, 2);
   }
@@ -485,7 +488,7 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
                             st));
     CUDA_OK(cudaMemsetAsync(nseeds + nseries + 1, 0, 4, st));
     ph.begin();
-    launch_seed_select(S, keys, seeds, nseeds, Q.bsf2, st);
+    launch_seed_select(S, keys, seeds, nseeds, Q.bsf2, st, false);
     DevSearch Qs = Q;
     Qs.qser = nullptr;
     Qs.queue_next = nseeds + nseries + 1;

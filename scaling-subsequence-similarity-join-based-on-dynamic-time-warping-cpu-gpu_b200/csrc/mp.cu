@@ -203,6 +203,137 @@ __global__ void __launch_bounds__(kLbThreads, 4) k_mp(DevSeries S, const Tile* t
   }
 }
 
+// Row minima for the join's seeds only.  The seeds choose which pairs get an
+// exact DTW first; nothing else depends on these keys' precision (the join's
+// starting best-so-far comes from those exact DTWs), so this pass keeps the
+// tile's exact FP64 anchor and carries the covariance in FP64 from stage to
+// stage, but accumulates the per-row increments of a stage (224 rows) in
+// FP32 on FP32 copies of the update terms.  On random walks that leaves ED^2
+// within about 1e-4 of the FP64 recurrence; the keys keep 20 mantissa bits.
+struct MpSeedShared {
+  float p1[kCols], p2[kCols], is[kCols], c2[kCols];
+  float r1[kStage], r2[kStage], ci[kStage];
+  unsigned long long rowbest[kStage];
+};
+
+__global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Tile* tiles,
+                                                           unsigned long long* keys) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  MpSeedShared& sh = *reinterpret_cast<MpSeedShared*>(smraw);
+  const Tile T = tiles[blockIdx.x];
+  const int64_t s = T.send;
+  const int m = S.m;
+  const int t = threadIdx.x, lane = t & 31;
+  const int64_t L0 = T.L0, i0 = T.i0;
+  const int64_t Lt = L0 + (int64_t)t * kLbPerThread;
+  // exact anchors C(i0, i0 + L) for the thread's lags (FP64)
+  double C[kLbPerThread];
+  {
+    double mj[kLbPerThread], wa[kLbPerThread];
+    const int64_t jb = i0 + Lt;
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) {
+      C[l] = 0.0;
+      mj[l] = S.mu[jb + l < s ? jb + l : s - 1];
+      wa[l] = S.a[jb + l < S.n ? jb + l : S.n - 1];
+    }
+    const double mi = S.mu[i0];
+    for (int k = 0; k < m; ++k) {
+      const double ai = S.a[i0 + k] - mi;
+#pragma unroll
+      for (int l = 0; l < kLbPerThread; ++l) C[l] = fma(ai, wa[l] - mj[l], C[l]);
+#pragma unroll
+      for (int l = 0; l < kLbPerThread - 1; ++l) wa[l] = wa[l + 1];
+      const int64_t x = jb + kLbPerThread + k < S.n ? jb + kLbPerThread + k : S.n - 1;
+      wa[kLbPerThread - 1] = S.a[x];
+    }
+  }
+  float w1[kLbPerThread], w2[kLbPerThread], wi[kLbPerThread], wc[kLbPerThread];
+  const float two_m = 2.0f * (float)m;
+  const unsigned int kReal = __float_as_uint(1e20f);  // above: a guard column, not a pair
+  for (int st = 0; st < T.rows; st += kStage) {
+    const int64_t r0 = i0 + st, c0 = r0 + L0;
+    __syncthreads();
+    for (int x = t; x < kStage; x += kLbThreads) sh.rowbest[x] = ULLONG_MAX;
+    for (int x = t; x < kCols; x += kLbThreads) {
+      const int64_t j = c0 + x;
+      const bool in = j >= 0 && j < s, up = j >= 1 && j < s;
+      sh.p1[x] = up ? (float)S.dfa[j - 1] : 0.0f;
+      sh.p2[x] = up ? (float)S.dga[j - 1] : 0.0f;
+      sh.is[x] = in ? (float)S.isg[j] : 0.0f;
+      sh.c2[x] = (in && !S.flat[j]) ? two_m : 1e30f;
+    }
+    for (int x = t; x < kStage; x += kLbThreads) {
+      const int64_t i = r0 + x;
+      const bool in = i >= 0 && i < s, up = i >= 1 && i < s;
+      sh.r1[x] = up ? (float)S.dfa[i - 1] : 0.0f;
+      sh.r2[x] = up ? (float)S.dga[i - 1] : 0.0f;
+      sh.ci[x] = (in && !S.flat[i]) ? (float)(-2.0 * S.isg[i]) : 0.0f;
+    }
+    __syncthreads();
+    const int cb = t * kLbPerThread;
+    float Cb[kLbPerThread], D[kLbPerThread];
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) {
+      w1[l] = sh.p1[cb + l];
+      w2[l] = sh.p2[cb + l];
+      wi[l] = sh.is[cb + l];
+      wc[l] = sh.c2[cb + l];
+      Cb[l] = (float)C[l];
+      D[l] = 0.0f;
+    }
+    for (int qq = 0; qq < kStage / kLbPerThread; ++qq) {
+#pragma unroll
+      for (int u = 0; u < kLbPerThread; ++u) {
+        const int r = qq * kLbPerThread + u;
+        const int64_t i = r0 + r;
+        const bool first = (st == 0 && r == 0);
+        const float q1 = sh.r1[r], q2 = sh.r2[r], qc = sh.ci[r];
+        const bool row_ok = (st + r < T.rows) && qc != 0.0f;
+        unsigned int best = UINT_MAX;
+#pragma unroll
+        for (int l = 0; l < kLbPerThread; ++l) {
+          const int sl = (u + l) % kLbPerThread;
+          if (!first) {
+            D[l] = fmaf(q1, w2[sl], D[l]);
+            D[l] = fmaf(w1[sl], q2, D[l]);
+          }
+          const float e2 = fmaxf(fmaf((Cb[l] + D[l]) * qc, wi[sl], wc[sl]), 0.0f);
+          best = min(best, (__float_as_uint(e2) & ~7u) | (unsigned int)l);
+        }
+        const int nx = cb + r + kLbPerThread;
+        w1[u] = sh.p1[nx];
+        w2[u] = sh.p2[nx];
+        wi[u] = sh.is[nx];
+        wc[u] = sh.c2[nx];
+        if (row_ok) {
+          const unsigned int wbest = __reduce_min_sync(0xffffffffu, best);
+          if (wbest < kReal) {
+            const unsigned int ballot = __ballot_sync(0xffffffffu, best == wbest);
+            if (lane == __ffs(ballot) - 1) {
+              // the float (20 mantissa bits kept) in the FP64 key format
+              const unsigned int hi =
+                  (unsigned int)__double2hiint((double)__uint_as_float(wbest & ~7u));
+              const unsigned long long key =
+                  ((unsigned long long)(hi & ~7u) << 32) |
+                  (unsigned long long)(unsigned int)(i + Lt + (wbest & 7u));
+              atomicMin(&sh.rowbest[r], key);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int l = 0; l < kLbPerThread; ++l) C[l] += (double)D[l];
+    __syncthreads();
+    const int nrow = T.rows - st < kStage ? T.rows - st : kStage;
+    for (int x = t; x < nrow; x += kLbThreads) {
+      const unsigned long long v = sh.rowbest[x];
+      if (v != ULLONG_MAX) atomicMin(&keys[r0 + x], v);
+    }
+  }
+}
+
 // Per tile, an upper bound on its smallest squared DTW distance: the ED^2 of
 // its closest pair (ED >= DTW), from the truncated key rounded up.
 __global__ void k_tile_bound(const unsigned int* tile_best, int ntiles, unsigned int* bsf2) {
@@ -325,7 +456,7 @@ constexpr int kLocal = 8;
 __global__ void __launch_bounds__(kSelThreads) k_seed_select(DevSeries S,
                                                               const unsigned long long* keys,
                                                               int2* seeds, unsigned int* nseeds,
-                                                              unsigned int* bsf2) {
+                                                              unsigned int* bsf2, bool key_bound) {
   // block b selects the seeds of series b (windows [wb, we))
   const int b = blockIdx.x;
   const int64_t wb = S.sbeg ? S.sbeg[b] : 0;
@@ -395,7 +526,7 @@ __global__ void __launch_bounds__(kSelThreads) k_seed_select(DevSeries S,
       for (int q = 0; q < kLocal; ++q) if (q == head) pj = part[q];
       const int i = (int)(wn & 0xffffffffu);
       seeds[round] = make_int2(i < pj ? i : pj, i < pj ? pj : i);
-      if (round == 0) {
+      if (round == 0 && key_bound) {
         // rounded up past the 3 cleared low bits of the key: ED^2 >= DTW^2
         const unsigned long long bits = (((wn >> 32) & ~7ull) + 8ull) << 32;
         const float e2 = __double2float_ru(__longlong_as_double((long long)bits));
@@ -440,6 +571,19 @@ void launch_mp(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long 
   }
 }
 
+void launch_mp_seed(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long long* keys,
+                    cudaStream_t st) {
+  k_fill_u64<<<1024, 256, 0, st>>>(keys, S.s, ULLONG_MAX);
+  if (ntiles <= 0) return;
+  cudaFuncSetAttribute(k_mp_seed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(MpSeedShared));
+  const int slab = 1 << 20;
+  for (int b = 0; b < ntiles; b += slab) {
+    const int cnt = ntiles - b < slab ? ntiles - b : slab;
+    k_mp_seed<<<cnt, kLbThreads, sizeof(MpSeedShared), st>>>(S, tiles + b, keys);
+  }
+}
+
 void launch_mp_collect(const DevSeries& S, const Tile* tiles, int ntiles,
                        const unsigned long long* want, int2* cand, unsigned int* count,
                        unsigned int cap, cudaStream_t st) {
@@ -478,8 +622,9 @@ void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
 }
 
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
-                        unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st) {
-  k_seed_select<<<S.nseries, kSelThreads, 0, st>>>(S, keys, seeds, nseeds, bsf2);
+                        unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st,
+                        bool key_bound) {
+  k_seed_select<<<S.nseries, kSelThreads, 0, st>>>(S, keys, seeds, nseeds, bsf2, key_bound);
 }
 
 }  // namespace dtwj
