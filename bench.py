@@ -319,8 +319,12 @@ def run_ours(args):
         raise SystemExit("bench.py needs torch with CUDA for device buffers")
     ctx = dtwj.Context(local)
     if world > 1:
-        # one join spread over the ranks: rank r sweeps the tiles t % world == r
+        # one join spread over the ranks: rank r sweeps the tiles t % world == r,
+        # and after each of 8 sweep phases the ranks lower their best-so-far to
+        # the smallest any rank has found (an NCCL all-reduce of one word on the
+        # join's stream); every rank runs the same joins, so the same collectives
         ctx.set_shard(rank, world)
+        ctx.set_exchange(dtwj.make_exchange(None, local), 8)
     # F_PROFILE records CUDA events around every launch group on the join's
     # stream (no synchronisation), so the timed joins also give the per-phase
     # device times the roofline uses.
