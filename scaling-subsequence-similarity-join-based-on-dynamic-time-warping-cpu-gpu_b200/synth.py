@@ -111,6 +111,10 @@ def workload(name: str):
         x = random_walk(262_144, 3)
         r = 0.1 if name.endswith("w52") else 0.2
         return dict(series=x, m=512, w=band(512, r), ratio=r)
+    if name in ("ecg16k_w52", "ecg16k_w103"):  # the first 16,384 samples of ecg262k_*
+        x = ecg_like(262_144, 3)[:16_384].copy()
+        r = 0.1 if name.endswith("w52") else 0.2
+        return dict(series=x, m=512, w=band(512, r), ratio=r)
     if name in ("ecg262k_w52", "ecg262k_w103"):
         x = ecg_like(262_144, 3)
         r = 0.1 if name.endswith("w52") else 0.2
