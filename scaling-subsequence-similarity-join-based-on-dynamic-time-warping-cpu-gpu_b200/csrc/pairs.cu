@@ -87,10 +87,47 @@ __host__ __device__ inline GroupLayout group_layout(int m, int w, int C, int G, 
   return l;
 }
 
-// Banded DTW of q (rows) against t (columns), squared cost.  With ABANDON the
-// group stops as soon as every lane's latest row, plus the cumulative bound
-// of the rows and columns still ahead, exceeds the threshold; it then returns
-// +inf and reports the cells it swept.
+// One row step of a lane: row tau - g of its C diagonals from `in` (the row
+// above) into `out`.  Cell (r, d) takes the minimum of (r, d-1) (the cell to
+// its left: out[c-1], or the left lane's last cell of the previous step),
+// (r-1, d) (in[c]) and (r-1, d+1) (in[c+1], or the right lane's first cell of
+// this step), plus (q[r] - t[r + d])^2; pen[c] is +inf for diagonals past the
+// band.  q and t are read from shared memory at immediate offsets (qg[tau],
+// tg[tau + c]), so no register window has to be shifted.
+template <typename T, int C, int G>
+__device__ __forceinline__ void band_step(const T* __restrict__ qg, const T* __restrict__ tg,
+                                          int tau, int g, unsigned int gm, T INF,
+                                          const T (&pen)[C], const T (&in)[C], T (&out)[C],
+                                          T& last) {
+  T left = __shfl_up_sync(gm, last, 1, G);
+  if (g == 0) left = INF;
+  const T qr = qg[tau];
+  const T* tp = tg + tau;
+  {
+    const T d = qr - tp[0];
+    const T v = fmin3_(in[1 < C ? 1 : 0], in[0], left);
+    out[0] = fmax_(fma(d, d, v), pen[0]);
+  }
+  T right = __shfl_down_sync(gm, out[0], 1, G);
+  if (g == G - 1) right = INF;
+#pragma unroll
+  for (int c = 1; c < C; ++c) {
+    const T up = (c + 1 < C) ? in[c + 1 < C ? c + 1 : 0] : right;
+    const T d = qr - tp[c];
+    const T v = fmin3_(up, in[c], out[c - 1]);
+    out[c] = fmax_(fma(d, d, v), pen[c]);
+  }
+  last = out[C - 1];
+}
+
+// Banded DTW of q (rows) against t (columns), squared cost.  A group of G
+// lanes computes one pair; lane g owns the C consecutive diagonals
+// d = -w + gC .. -w + gC + C - 1 and handles row tau - g at step tau.  The
+// first G steps (the lanes starting one after another) keep a lane's row
+// until it reaches row 0; after them two row buffers alternate, two steps per
+// iteration.  With ABANDON the group checks every 16 steps whether every
+// lane's latest row, plus the cumulative bound of the rows still ahead,
+// exceeds the threshold; it then returns +inf and reports the cells it swept.
 template <typename T, int C, int G, bool ABANDON>
 __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, int w,
                       const float* __restrict__ cbc, int nc, float thr,
@@ -98,71 +135,42 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
                       unsigned long long* cells, bool* abandoned) {
   const T INF = Pad<T>::inf();
   const int d_lo = -w + g * C;
-  T pen[C], prev[C], cur[C], tw[C];
+  T pen[C], A[C], B[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) {
     pen[c] = (d_lo + c <= w) ? T(0) : INF;
-    prev[c] = (d_lo + c == 0) ? T(0) : INF;
-    tw[c] = t[-g + d_lo + c];
+    A[c] = (d_lo + c == 0) ? T(0) : INF;  // virtual row -1: D(-1, 0) = 0
   }
+  const T* qg = q - g;         // qg[tau] = q[row]
+  const T* tg = t - g + d_lo;  // tg[tau + c] = t[row + d_lo + c]
   const int g0 = w / C, c0 = w % C;
-  const int tau_end = m - 1 + g0;
+  const int tau_end = m - 1 + g0;  // lane g0 (cell c0 on d = 0) reaches row m - 1
   T last = INF;
-  T result = INF;
   *abandoned = false;
-#pragma unroll 2
-  for (int tau = 0; tau <= tau_end; ++tau) {
-    const int r = tau - g;
-    T left = __shfl_up_sync(gm, last, 1, G);
-    if (g == 0) left = INF;
-    const T qr = q[r];
-    {
-      const T d = qr - tw[0];
-      T v = fmin3_(prev[1 < C ? 1 : 0], prev[0], left);
-      v = fmax_(fma(d, d, v), pen[0]);
-      cur[0] = v;
-    }
-    T right = __shfl_down_sync(gm, cur[0], 1, G);
-    if (g == G - 1) right = INF;
+  // warm-up: a lane that has not reached row 0 keeps its initial row
+  const int warm = G < tau_end + 1 ? G : tau_end + 1;
+  for (int tau = 0; tau < warm; ++tau) {
+    band_step<T, C, G>(qg, tg, tau, g, gm, INF, pen, A, B, last);
+    const bool live = tau - g >= 0;
 #pragma unroll
-    for (int c = 1; c < C; ++c) {
-      const T up = (c + 1 < C) ? prev[c + 1 < C ? c + 1 : 0] : right;
-      const T d = qr - tw[c];
-      T v = fmin3_(up, prev[c], cur[c - 1]);
-      v = fmax_(fma(d, d, v), pen[c]);
-      cur[c] = v;
-    }
-    last = cur[C - 1];
-    if (tau == tau_end && g == g0) {
+    for (int c = 0; c < C; ++c) A[c] = live ? B[c] : A[c];
+  }
+  int tau = warm;
+  while (tau < tau_end) {  // two steps left at least
+    band_step<T, C, G>(qg, tg, tau, g, gm, INF, pen, A, B, last);
+    band_step<T, C, G>(qg, tg, tau + 1, g, gm, INF, pen, B, A, last);
+    tau += 2;
+    if (ABANDON && ((tau - warm) & 15) == 0 && tau <= tau_end) {
+      const int r = tau - 1 - g;  // this lane's latest row
+      T fm = A[0];
 #pragma unroll
-      for (int c = 0; c < C; ++c)
-        if (c == c0) result = cur[c];
-    }
-    if (tau < G) {
-      // warm-up: a lane that has not reached row 0 keeps its initial row
-      // (which holds the virtual start D(-1, 0) = 0 for the lane owning d = 0)
-      const bool live = r >= 0;
-#pragma unroll
-      for (int c = 0; c < C; ++c) prev[c] = live ? cur[c] : prev[c];
-    } else {
-#pragma unroll
-      for (int c = 0; c < C; ++c) prev[c] = cur[c];
-    }
-#pragma unroll
-    for (int c = 0; c < C - 1; ++c) tw[c] = tw[c + 1];
-    tw[C - 1] = t[r + d_lo + C];
-    if (ABANDON && (tau & 15) == 15 && tau >= G && tau < tau_end) {
-      T fm = cur[0];
-#pragma unroll
-      for (int c = 1; c < C; ++c) fm = fmin_(fm, cur[c]);
+      for (int c = 1; c < C; ++c) fm = fmin_(fm, A[c]);
       int idx = r + w + 1;
       idx = idx < 0 ? 0 : (idx + 7) >> 3;
       const float cbv = cbc[idx < nc ? idx : nc];
-      const float fresh = prune_threshold_now(bsf2, m);
-      thr = fminf(thr, fresh);
+      thr = fminf(thr, prune_threshold_now(bsf2, m));
       const bool over = (float)fm + cbv > thr;
-      const unsigned int vote = __ballot_sync(gm, over);
-      if ((vote & gm) == gm) {
+      if ((__ballot_sync(gm, over) & gm) == gm) {
         // cells swept so far: rows [0, rows_done) of each owned diagonal
         const int rows_done = r + 1 < 0 ? 0 : (r + 1 > m ? m : r + 1);
         unsigned long long cnt = 0;
@@ -180,6 +188,15 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
       }
     }
   }
+  if (tau == tau_end) {  // an odd last step
+    band_step<T, C, G>(qg, tg, tau, g, gm, INF, pen, A, B, last);
+#pragma unroll
+    for (int c = 0; c < C; ++c) A[c] = B[c];
+  }
+  T result = INF;
+#pragma unroll
+  for (int c = 0; c < C; ++c)
+    if (c == c0) result = A[c];
   result = __shfl_sync(gm, result, g0, G);
   *cells = (unsigned long long)m * (2 * w + 1) - (unsigned long long)w * (w + 1);
   return result;
