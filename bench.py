@@ -402,15 +402,18 @@ def run_ours(args):
     #   k_lb    reads the six per-index FP64 operands of its rows and columns
     #           ((2 rows + 896 lags) x 48 B per tile) and writes the survivor
     #           bits (896 lags x 126 words x 4 B per tile)
-    #   k_runs  reads those bits and writes one 16-byte LB_Keogh candidate per
-    #           pair that passes the masked and endpoint bounds
+    #   k_paa   reads those bits and the 16-byte block means of the windows a
+    #           tile covers (rows + 896 lags + m samples per tile), and writes
+    #           one 16-byte LB_Keogh candidate per pair that passes the
+    #           block-mean and endpoint bounds (k_runs, the masked cascade's
+    #           filter, in its place under F_MASKED_CASCADE)
     #   k_keogh reads the candidates and writes an 8-byte DTW entry per survivor
     ntiles, rows_sum = sweep_tiles(n, m)
     bits_bytes = ntiles * 896 * 126 * 4
     kq_entries = r0.pruned_keogh + r0.dtw_calls  # pairs that reached LB_Keogh (seeds aside)
     alg = {
         "diag": ("k_lb", (2 * rows_sum + ntiles * 896) * 48 + bits_bytes),
-        "runs": ("k_runs", bits_bytes + 16 * kq_entries),
+        "runs": ("k_paa", bits_bytes + 16 * (rows_sum + ntiles * (896 + m)) + 16 * kq_entries),
         "keogh": ("k_keogh", 16 * kq_entries + 8 * r0.dtw_calls),
     }
     sweep_phases = [p for p in ("runs", "keogh", "diag") if phases.get(p, 0) > 0]

@@ -45,6 +45,22 @@ __device__ __forceinline__ bool fp32_bound_ok(float r, float thr, int m) {
   return err <= slack;
 }
 
+// The largest error scale r for which fp32_bound_ok(r, thr, m) holds (the
+// error bound is increasing in r): the positive root of
+// a r^2 + b r + c = 0 with a = m k^2, b = 2 k sqrt(m thr), c = summation term
+// - slack, k = 16 * 2^-24, in the form -2c / (b + sqrt(b^2 - 4ac)) that does
+// not cancel, shrunk by 2^-10 against the rounding of this evaluation; -1 if
+// none.
+__device__ __forceinline__ float fp32_bound_radius(float thr, int m) {
+  const float fm = (float)m, k = 16.0f / 16777216.0f;
+  const float slack = (thr * kSlack + kAbsSlackPerSample * fm) * (1.0f / (1.0f + kSlack));
+  const float c = thr * ((fm * 0.125f + 8.0f) * (1.0f / 16777216.0f)) - slack;
+  if (!(c < 0.0f)) return -1.0f;  // also +inf / NaN thresholds: no FP32 pruning
+  const float a = fm * k * k, b = 2.0f * k * sqrtf(fm * thr);
+  const float r = -2.0f * c / (b + sqrtf(b * b - 4.0f * a * c));
+  return r * (1.0f - 1.0f / 1024.0f);
+}
+
 // Endpoint bound width (the reference's BIAS, CPU_version1/diag_mask_global.cpp:8).
 constexpr int kBias = 3;
 // Seeds taken from the ED matrix profile (CPU_version1/new_dtw_motifGUI.cpp:53).

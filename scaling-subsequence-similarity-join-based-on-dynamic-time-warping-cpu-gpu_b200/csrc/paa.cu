@@ -160,27 +160,41 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 3) k_paa(DevSeries S, DevSearc
     if (!nz) continue;
     const Tile T = tiles[tk];
     const unsigned int* bsf2 = Q.bsf2 + T.series;
-    const int64_t ib = (int64_t)T.i0 + wi * 32;  // the batch's first row
+    // positions fit 32 bits (n <= INT32_MAX - 4)
+    const int ib = T.i0 + wi * 32;  // the batch's first row
+    const int i_row = ib + lane;    // this lane's row
     // aligned blocks inside every row's window [ib + p, ib + p + m), p < 32
     // (none when m is short: each lane then covers its window by itself)
-    int64_t x_lo = (ib + 31 + B - 1) / B * B, x_hi = (ib + m) / B * B;
+    int x_lo = (ib + 31 + B - 1) / B * B, x_hi = (ib + m) / B * B;
     const bool shared = x_lo < x_hi;
     if (!shared) x_lo = x_hi = 0;
+    // the threshold, once per item (a later, lower best-so-far only prunes
+    // more: the one read here stays valid), and the largest error scale
+    // whose FP32 bound may prune against it
+    const float thr = prune_threshold_now(bsf2, m);
+    const float r_ok = fp32_bound_radius(thr, m);
+    // the row side, the same for every lag of the item: window statistics and
+    // the offsets of the (at most two) 1024-blocks of the shared range
+    const int i_own = i_row < T.send ? i_row : T.send - 1;  // a valid row for the loads
+    const double mi_own = S.mu[i_own], si_own = S.isg[i_own];
+    // the error scale a partner may have and still prune with this row (-1: none)
+    const float r_lane = S.rw[i_own] <= r_ok ? r_ok : -1.0f;
+    const int b_lo = x_lo >> kBlkShift;
+    const double oi0_own = win_offset(S, b_lo, mi_own, si_own);
+    const double oi1_own = win_offset(S, b_lo + 1, mi_own, si_own);
     while (nz) {
       const int l = __ffs(nz) - 1;
       nz &= nz - 1u;
       const unsigned int wb = __shfl_sync(0xffffffffu, word, l);
       const bool live = (wb >> lane) & 1u;  // the sweep set only bits of valid pairs
-      const int64_t L = (int64_t)T.L0 + g * 32 + l;
+      const int L = T.L0 + g * 32 + l;
       // a lane without a pair computes the first live lane's pair (valid
       // addresses, result ignored), so the block loops need no predicate
       const int src = __ffs(wb) - 1;
-      const int64_t i = ib + (live ? lane : src), j = i + L;
-      const float thr = prune_threshold_now(bsf2, m);
-      const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
-      // a pair whose FP32 error bound does not fit the slack is never pruned here
-      const float thr_lane =
-          live && fp32_bound_ok(fmaxf(S.rw[i], S.rw[j]), thr, m) ? thr : __int_as_float(0x7f800000);
+      const int i = ib + (live ? lane : src), j = i + L;
+      const double mi = mi_own, si = si_own;  // a borrowed pair's are only approximate: ignored
+      const double mj = S.mu[j], sj = S.isg[j];
+      const float thr_lane = live && S.rw[j] <= r_lane ? thr : __int_as_float(0x7f800000);
       const float fsi = (float)si, fsj = (float)sj;
       float acc1 = 0.0f, acc2 = 0.0f;
       // ---- this lane's own blocks before and after the shared ones ----
@@ -188,15 +202,15 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 3) k_paa(DevSeries S, DevSearc
         // head [i, x_lo) and tail [x_hi, i + m) are each at most 30 + B
         // samples long; without shared blocks the head is the whole window
         // (m < 31 + 2B, so at most 2 (30 + B) / B blocks as well)
-        const int nh = shared ? (int)((x_lo - i) / B) : m / B;
-        const int nt = shared ? (int)((i + m - x_hi) / B) : 0;
+        const int nh = shared ? (x_lo - i) / B : m / B;
+        const int nt = shared ? (i + m - x_hi) / B : 0;
         constexpr int kEdgeMax = 2 * ((30 + B) / B);
 #pragma unroll 1
         for (int e = 0; e < kEdgeMax; ++e) {
           const bool head = e < nh, tail = e >= nh && e < nh + nt;
           if (head || tail) {
-            const int64_t xi = head ? i + (int64_t)e * B : x_hi + (int64_t)(e - nh) * B;
-            const int64_t xj = xi + L;
+            const int xi = head ? i + e * B : x_hi + (e - nh) * B;
+            const int xj = xi + L;
             const float o = (float)(win_offset(S, xi >> kBlkShift, mi, si) -
                                     win_offset(S, xj >> kBlkShift, mj, sj));
             block_terms(S.pq[xi], S.pq[xj], fsi, fsj, o, acc1, acc2);
@@ -205,18 +219,20 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 3) k_paa(DevSeries S, DevSearc
       }
       // ---- the shared aligned blocks, in segments of constant offsets ----
       bool pruned = !live || (float)B * fmaxf(acc1, acc2) > thr_lane;
-      int64_t x = x_lo;
+      int x = x_lo;
       while (x < x_hi && !__all_sync(0xffffffffu, pruned)) {
         // the next block whose i or j side starts in another 1024-sample block
-        const int64_t ci = (x / kSpan + 1) * kSpan;
-        const int64_t cj = ((((x + L) / kSpan + 1) * kSpan - L) + B - 1) / B * B;
-        int64_t seg = ci < cj ? ci : cj;
+        const int ci = ((x >> kBlkShift) + 1) << kBlkShift;
+        const int cj = (((((x + L) >> kBlkShift) + 1) << kBlkShift) - L + B - 1) / B * B;
+        int seg = ci < cj ? ci : cj;
         if (seg > x_hi) seg = x_hi;
-        const float oij = (float)(win_offset(S, x >> kBlkShift, mi, si) -
-                                  win_offset(S, (x + L) >> kBlkShift, mj, sj));
+        const int bx = x >> kBlkShift;
+        const double oi = bx == b_lo ? oi0_own
+                        : (bx == b_lo + 1 ? oi1_own : win_offset(S, bx, mi, si));
+        const float oij = (float)(oi - win_offset(S, (x + L) >> kBlkShift, mj, sj));
         const float4* qi = S.pq + x;
         const float4* qj = S.pq + x + L;
-        const int nblk = (int)((seg - x) / B);
+        const int nblk = (seg - x) / B;
         int k = 0;
         for (; k + 4 <= nblk; k += 4, qi += 4 * B, qj += 4 * B) {
 #pragma unroll
@@ -258,7 +274,7 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 3) k_paa(DevSeries S, DevSearc
         if (alive) {
           const unsigned int slot = base + __popc(sv & ((1u << lane) - 1u));
           if (slot < Q.kq_cap) {
-            Q.kq[slot] = make_int4((int)i, (int)j, __float_as_int(kim), T.series);
+            Q.kq[slot] = make_int4(i, j, __float_as_int(kim), T.series);
           } else {
             atomicOr(S.status, 2);
           }
