@@ -65,6 +65,11 @@ __device__ __forceinline__ float fp32_bound_radius(float thr, int m) {
 constexpr int kBias = 3;
 // Seeds taken from the ED matrix profile (CPU_version1/new_dtw_motifGUI.cpp:53).
 constexpr int kSeeds = 100;
+// The seed profile keys one row in kSeedGrid; each seed pair is widened to
+// kSeedSpread pairs on its diagonal (offsets -kSeedGrid/2 .. kSeedGrid/2).
+constexpr int kSeedGrid = 7;
+constexpr int kSeedSpread = kSeedGrid;
+constexpr int kSeedSlots = kSeeds * kSeedSpread;
 // Sentinels padding the z-normalised sequences: finite so that no
 // inf - inf appears, far enough apart that any cell touching them is
 // effectively infinite.
@@ -266,15 +271,14 @@ void launch_mp_exact(const DevSeries& S, const int2* cand, const unsigned int* c
 void launch_mp_exact_out(int64_t s, const unsigned long long* rowmin,
                          const unsigned long long* rowidx, double* mp, int64_t* mpi,
                          cudaStream_t st);
-// kSeeds seeds per series into seeds[series * kSeeds ...] (unused slots hold
-// (-1, -1)), their counts into nseeds[series] and the initial best-so-far
-// into bsf2[series].
-// key_bound: also set bsf2 from the best key (an exact FP64 profile only).
+// kSeeds seeds per series, each with its diagonal neighbours, into
+// seeds[series * kSeedSlots ...] (unused slots hold (-1, -1)), their counts
+// into nseeds[series].
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
-                        unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st,
-                        bool key_bound);
-// Row minima for the join's seeds: FP64 anchors and stage carries, FP32
-// increments within a stage (keys only rank the seed candidates).
+                        unsigned int* nseeds, cudaStream_t st);
+// Row minima for the join's seeds on the rows of a kSeedGrid grid: FP64
+// anchors and stage carries, FP32 increments within a stage (keys only rank
+// the seed candidates).
 void launch_mp_seed(const DevSeries& S, const Tile* tiles, int ntiles, unsigned long long* keys,
                     cudaStream_t st);
 // Series of a sample (0 for a single series).
@@ -296,9 +300,10 @@ void launch_runs(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int 
                  cudaStream_t st);
 void launch_center(const DevSeries& S, cudaStream_t st);
 // 64 features per tile for the learned ordering (features.cu), from the
-// profile keys of the series' rows; out[64 * t ...] for tile t.
+// profile keys of the series' rows (every row keyed: grid 1; the seed
+// profile: grid kSeedGrid); out[64 * t ...] for tile t.
 void launch_tile_features(const DevSeries& S, const Tile* tiles, int ntiles,
-                          const unsigned long long* keys, float* out, cudaStream_t st);
+                          const unsigned long long* keys, int grid, float* out, cudaStream_t st);
 // Block-mean lower bound (LB_PAA) over the survivor bits of LB tiles
 // [tile_begin, tile_end), then the endpoint bound; survivors go to Q.kq.
 void launch_paa(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,

@@ -49,7 +49,7 @@ __device__ __forceinline__ double mp_value(unsigned long long key, double inv_no
 }
 
 __global__ void k_tile_features(DevSeries S, const Tile* tiles, int ntiles,
-                                const unsigned long long* keys, float* out) {
+                                const unsigned long long* keys, int grid, float* out) {
   const int lane = threadIdx.x & 31;
   const int t = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
   if (t >= ntiles) return;
@@ -104,7 +104,10 @@ __global__ void k_tile_features(DevSeries S, const Tile* tiles, int ntiles,
     mn = wmin(mn);
     cnt = wsum(cnt);
     mpmin[k] = mn;
-    frac[k] = b > a ? cnt / (b - a) : 0.0;
+    // rows that carry a key: every row, or the rows r % grid == 0 of the seed
+    // profile's grid (a tile starts on its series' grid)
+    const int keyed = (b + grid - 1) / grid - (a + grid - 1) / grid;
+    frac[k] = keyed > 0 ? cnt / keyed : 0.0;
     tile_min = fmin(tile_min, mn);
   }
   // ED and LB_Keogh of 8 sample pairs at the middle lag
@@ -160,11 +163,12 @@ __global__ void k_tile_features(DevSeries S, const Tile* tiles, int ntiles,
 }  // namespace
 
 void launch_tile_features(const DevSeries& S, const Tile* tiles, int ntiles,
-                          const unsigned long long* keys, float* out, cudaStream_t st) {
+                          const unsigned long long* keys, int grid, float* out,
+                          cudaStream_t st) {
   if (ntiles <= 0) return;
   const int per_block = 4;  // warps
   k_tile_features<<<(ntiles + per_block - 1) / per_block, 32 * per_block, 0, st>>>(
-      S, tiles, ntiles, keys, out);
+      S, tiles, ntiles, keys, grid, out);
 }
 
 }  // namespace dtwj

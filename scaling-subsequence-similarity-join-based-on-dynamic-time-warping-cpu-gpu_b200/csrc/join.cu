@@ -433,8 +433,9 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
       CUDA_OK(cudaMemsetAsync(tbest, 0xff, (size_t)nlb * 4, st));
     }
     ph.begin();
-    // a join only ranks seed candidates by these keys (mixed precision); the
-    // per-tile minima and the exported features take the exact FP64 profile
+    // a join only ranks seed candidates by these keys (mixed precision, one
+    // row in kSeedGrid); the per-tile minima and the exported features take
+    // the exact FP64 profile of every row
     if (tq) launch_mp(S, lbtiles, nlb, keys, st, tbest);
     else launch_mp_seed(S, lbtiles, nlb, keys, st);
     if (tile_mode) launch_tile_bound(tbest, nlb, Q.bsf2, st);
@@ -444,7 +445,7 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   if (want_features && nlb > 0) {
     float* feat;
     ENSURE(B_FEAT, (size_t)nlb * DTWJ_MLP_IN * 4, feat);
-    launch_tile_features(S, lbtiles, nlb, keys, feat, st);
+    launch_tile_features(S, lbtiles, nlb, keys, tq ? 1 : kSeedGrid, feat, st);
     if (tq && tq->features)
       CUDA_OK(cudaMemcpyAsync(tq->features, feat, (size_t)nlb * DTWJ_MLP_IN * 4,
                               cudaMemcpyDeviceToHost, st));
@@ -481,18 +482,18 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   if (!tile_mode && !(flags & DTWJ_F_NO_SEED) && nlb > 0) {
     int2* seeds;
     unsigned int* nseeds;  // [nseries] counts, total slots, work counter
-    ENSURE(B_SEEDS, (size_t)nseries * kSeeds * sizeof(int2), seeds);
+    ENSURE(B_SEEDS, (size_t)nseries * kSeedSlots * sizeof(int2), seeds);
     ENSURE(B_NSEEDS, ((size_t)nseries + 2) * 4, nseeds);
-    ctx->host_u32[0] = (unsigned int)(nseries * kSeeds);
+    ctx->host_u32[0] = (unsigned int)(nseries * kSeedSlots);
     CUDA_OK(cudaMemcpyAsync(nseeds + nseries, ctx->host_u32.data(), 4, cudaMemcpyHostToDevice,
                             st));
     CUDA_OK(cudaMemsetAsync(nseeds + nseries + 1, 0, 4, st));
     ph.begin();
-    launch_seed_select(S, keys, seeds, nseeds, Q.bsf2, st, false);
+    launch_seed_select(S, keys, seeds, nseeds, st);
     DevSearch Qs = Q;
     Qs.qser = nullptr;
     Qs.queue_next = nseeds + nseries + 1;
-    Qs.queue_cap = (unsigned int)(nseries * kSeeds);
+    Qs.queue_cap = (unsigned int)(nseries * kSeedSlots);
     launch_pairs(S, Qs, seeds, nseeds + nseries, false, band, ctx->num_sms, st);
     ph.end(DTWJ_PHASE_SEEDS, 2);
   }

@@ -204,16 +204,27 @@ __global__ void __launch_bounds__(kLbThreads, 4) k_mp(DevSeries S, const Tile* t
 }
 
 // Row minima for the join's seeds only.  The seeds choose which pairs get an
-// exact DTW first; nothing else depends on these keys' precision (the join's
-// starting best-so-far comes from those exact DTWs), so this pass keeps the
-// tile's exact FP64 anchor and carries the covariance in FP64 from stage to
-// stage, but accumulates the per-row increments of a stage (224 rows) in
-// FP32 on FP32 copies of the update terms.  On random walks that leaves ED^2
-// within about 1e-4 of the FP64 recurrence; the keys keep 20 mantissa bits.
+// exact DTW first; nothing else depends on these keys (the join's starting
+// best-so-far comes from those exact DTWs, and the result never depends on
+// it), so this pass samples and approximates:
+//  - only the rows on a grid of kSeedGrid rows (i - i0 a multiple of
+//    kSeedGrid; every tile starts on the grid of its series) get a key.  The
+//    covariance recurrence still steps every row, but the ED^2, the minimum
+//    and the row reduction run on one row in kSeedGrid.  A seed (i, j) is
+//    later widened to its diagonal neighbours (i + d, j + d), |d| <=
+//    kSeedGrid / 2, which covers every row of the grid cell;
+//  - the pass keeps the tile's exact FP64 anchor and carries the covariance
+//    in FP64 from stage to stage, but accumulates the per-row increments of a
+//    stage (224 rows) in FP32 on FP32 copies of the update terms.  On random
+//    walks that leaves ED^2 within about 1e-4 of the FP64 recurrence; the keys
+//    keep 20 mantissa bits.
+static_assert(kSeedGrid == kLbPerThread, "grid rows are the first of each unrolled group");
+static_assert(kLbRows % kSeedGrid == 0 && kStage % kSeedGrid == 0, "tiles and stages on the grid");
+
 struct MpSeedShared {
   float p1[kCols], p2[kCols], is[kCols], c2[kCols];
   float r1[kStage], r2[kStage], ci[kStage];
-  unsigned long long rowbest[kStage];
+  unsigned long long rowbest[kStage / kSeedGrid];
 };
 
 __global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Tile* tiles,
@@ -248,13 +259,13 @@ __global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Ti
       wa[kLbPerThread - 1] = S.a[x];
     }
   }
-  float w1[kLbPerThread], w2[kLbPerThread], wi[kLbPerThread], wc[kLbPerThread];
+  float w1[kLbPerThread], w2[kLbPerThread];
   const float two_m = 2.0f * (float)m;
   const unsigned int kReal = __float_as_uint(1e20f);  // above: a guard column, not a pair
   for (int st = 0; st < T.rows; st += kStage) {
     const int64_t r0 = i0 + st, c0 = r0 + L0;
     __syncthreads();
-    for (int x = t; x < kStage; x += kLbThreads) sh.rowbest[x] = ULLONG_MAX;
+    for (int x = t; x < kStage / kSeedGrid; x += kLbThreads) sh.rowbest[x] = ULLONG_MAX;
     for (int x = t; x < kCols; x += kLbThreads) {
       const int64_t j = c0 + x;
       const bool in = j >= 0 && j < s, up = j >= 1 && j < s;
@@ -277,8 +288,6 @@ __global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Ti
     for (int l = 0; l < kLbPerThread; ++l) {
       w1[l] = sh.p1[cb + l];
       w2[l] = sh.p2[cb + l];
-      wi[l] = sh.is[cb + l];
-      wc[l] = sh.c2[cb + l];
       Cb[l] = (float)C[l];
       D[l] = 0.0f;
     }
@@ -286,27 +295,27 @@ __global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Ti
 #pragma unroll
       for (int u = 0; u < kLbPerThread; ++u) {
         const int r = qq * kLbPerThread + u;
-        const int64_t i = r0 + r;
         const bool first = (st == 0 && r == 0);
-        const float q1 = sh.r1[r], q2 = sh.r2[r], qc = sh.ci[r];
-        const bool row_ok = (st + r < T.rows) && qc != 0.0f;
-        unsigned int best = UINT_MAX;
+        const float q1 = sh.r1[r], q2 = sh.r2[r];
+        if (!first) {
 #pragma unroll
-        for (int l = 0; l < kLbPerThread; ++l) {
-          const int sl = (u + l) % kLbPerThread;
-          if (!first) {
+          for (int l = 0; l < kLbPerThread; ++l) {
+            const int sl = (u + l) % kLbPerThread;  // ring slot of lag l at this row
             D[l] = fmaf(q1, w2[sl], D[l]);
             D[l] = fmaf(w1[sl], q2, D[l]);
           }
-          const float e2 = fmaxf(fmaf((Cb[l] + D[l]) * qc, wi[sl], wc[sl]), 0.0f);
-          best = min(best, (__float_as_uint(e2) & ~7u) | (unsigned int)l);
         }
-        const int nx = cb + r + kLbPerThread;
-        w1[u] = sh.p1[nx];
-        w2[u] = sh.p2[nx];
-        wi[u] = sh.is[nx];
-        wc[u] = sh.c2[nx];
-        if (row_ok) {
+        // a grid row (u == 0: lag l's column sits in ring slot l and at
+        // stage column cb + r + l)
+        const float qc = sh.ci[r];
+        if (u == 0 && st + r < T.rows && qc != 0.0f) {
+          unsigned int best = UINT_MAX;
+#pragma unroll
+          for (int l = 0; l < kLbPerThread; ++l) {
+            const float e2 =
+                fmaxf(fmaf((Cb[l] + D[l]) * qc, sh.is[cb + r + l], sh.c2[cb + r + l]), 0.0f);
+            best = min(best, (__float_as_uint(e2) & ~7u) | (unsigned int)l);
+          }
           const unsigned int wbest = __reduce_min_sync(0xffffffffu, best);
           if (wbest < kReal) {
             const unsigned int ballot = __ballot_sync(0xffffffffu, best == wbest);
@@ -316,20 +325,23 @@ __global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Ti
                   (unsigned int)__double2hiint((double)__uint_as_float(wbest & ~7u));
               const unsigned long long key =
                   ((unsigned long long)(hi & ~7u) << 32) |
-                  (unsigned long long)(unsigned int)(i + Lt + (wbest & 7u));
-              atomicMin(&sh.rowbest[r], key);
+                  (unsigned long long)(unsigned int)(r0 + r + Lt + (wbest & 7u));
+              atomicMin(&sh.rowbest[r / kSeedGrid], key);
             }
           }
         }
+        const int nx = cb + r + kLbPerThread;
+        w1[u] = sh.p1[nx];
+        w2[u] = sh.p2[nx];
       }
     }
 #pragma unroll
     for (int l = 0; l < kLbPerThread; ++l) C[l] += (double)D[l];
     __syncthreads();
     const int nrow = T.rows - st < kStage ? T.rows - st : kStage;
-    for (int x = t; x < nrow; x += kLbThreads) {
+    for (int x = t; x * kSeedGrid < nrow; x += kLbThreads) {
       const unsigned long long v = sh.rowbest[x];
-      if (v != ULLONG_MAX) atomicMin(&keys[r0 + x], v);
+      if (v != ULLONG_MAX) atomicMin(&keys[r0 + (int64_t)x * kSeedGrid], v);
     }
   }
 }
@@ -451,18 +463,18 @@ constexpr int kLocal = 8;
 
 // kSeeds smallest row minima (by ED^2 key, then row index).  Each thread
 // keeps the kLocal best of a strided slice; kSeeds rounds of block minimum
-// then pop the global order.  Writes the seed pairs, their count and the
-// initial best-so-far (the smallest ED^2, rounded up: ED >= DTW).
+// then pop the global order.  Writes each seed pair with its diagonal
+// neighbours (kSeedSpread slots per seed, (-1, -1) where a neighbour leaves
+// the series) and the seed count.
 __global__ void __launch_bounds__(kSelThreads) k_seed_select(DevSeries S,
                                                               const unsigned long long* keys,
-                                                              int2* seeds, unsigned int* nseeds,
-                                                              unsigned int* bsf2, bool key_bound) {
+                                                              int2* seeds, unsigned int* nseeds) {
   // block b selects the seeds of series b (windows [wb, we))
   const int b = blockIdx.x;
   const int64_t wb = S.sbeg ? S.sbeg[b] : 0;
   const int64_t we = S.sbeg ? S.sbeg[b + 1] - S.m + 1 : S.s;
-  seeds += (size_t)b * kSeeds;
-  for (int x = threadIdx.x; x < kSeeds; x += blockDim.x) seeds[x] = make_int2(-1, -1);
+  seeds += (size_t)b * kSeedSlots;
+  for (int x = threadIdx.x; x < kSeedSlots; x += blockDim.x) seeds[x] = make_int2(-1, -1);
   unsigned long long loc[kLocal];
   int part[kLocal];
 #pragma unroll
@@ -525,12 +537,12 @@ __global__ void __launch_bounds__(kSelThreads) k_seed_select(DevSeries S,
 #pragma unroll
       for (int q = 0; q < kLocal; ++q) if (q == head) pj = part[q];
       const int i = (int)(wn & 0xffffffffu);
-      seeds[round] = make_int2(i < pj ? i : pj, i < pj ? pj : i);
-      if (round == 0 && key_bound) {
-        // rounded up past the 3 cleared low bits of the key: ED^2 >= DTW^2
-        const unsigned long long bits = (((wn >> 32) & ~7ull) + 8ull) << 32;
-        const float e2 = __double2float_ru(__longlong_as_double((long long)bits));
-        bsf2[b] = __float_as_uint(e2);
+      const int lo = i < pj ? i : pj, hi = i < pj ? pj : i;
+      // the pair and its diagonal neighbours that lie in the series
+      for (int d = 0; d < kSeedSpread; ++d) {
+        const int off = d - kSeedSpread / 2;
+        const bool ok = lo + off >= wb && hi + off < we;
+        seeds[round * kSeedSpread + d] = ok ? make_int2(lo + off, hi + off) : make_int2(-1, -1);
       }
       ++head;
     }
@@ -622,9 +634,8 @@ void launch_mp_finalize(const DevSeries& S, const unsigned long long* up,
 }
 
 void launch_seed_select(const DevSeries& S, const unsigned long long* keys, int2* seeds,
-                        unsigned int* nseeds, unsigned int* bsf2, cudaStream_t st,
-                        bool key_bound) {
-  k_seed_select<<<S.nseries, kSelThreads, 0, st>>>(S, keys, seeds, nseeds, bsf2, key_bound);
+                        unsigned int* nseeds, cudaStream_t st) {
+  k_seed_select<<<S.nseries, kSelThreads, 0, st>>>(S, keys, seeds, nseeds);
 }
 
 }  // namespace dtwj

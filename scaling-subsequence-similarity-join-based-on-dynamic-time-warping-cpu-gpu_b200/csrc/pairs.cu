@@ -83,59 +83,68 @@ __host__ __device__ inline GroupLayout group_layout(int m, int w, int C, int G, 
   l.t_off = l.pq + m + l.pq + l.pt;
   l.cb_off = l.t_off + m + l.pt;
   l.total = l.cb_off + l.nc + 2;
-  l.total = (l.total + 3) & ~3;
+  // groups of a warp read their own q and t at a stride of C - 1 floats per
+  // lane: an odd group stride (17 mod 32) keeps two groups off each other's
+  // shared-memory banks
+  l.total = l.total + ((17 - l.total % 32) + 32) % 32;
   return l;
 }
 
-// One row step of a lane: row tau - g of its C diagonals from `in` (the row
-// above) into `out`.  Cell (r, d) takes the minimum of (r, d-1) (the cell to
-// its left: out[c-1], or the left lane's last cell of the previous step),
-// (r-1, d) (in[c]) and (r-1, d+1) (in[c+1], or the right lane's first cell of
-// this step), plus (q[r] - t[r + d])^2; pen[c] is +inf for diagonals past the
-// band.  q and t are read from shared memory at immediate offsets (qg[tau],
-// tg[tau + c]), so no register window has to be shifted.
-template <typename T, int C, int G>
-__device__ __forceinline__ void band_step(const T* __restrict__ qg, const T* __restrict__ tg,
-                                          int tau, int g, unsigned int gm, T INF,
-                                          const T (&pen)[C], const T (&in)[C], T (&out)[C],
-                                          T& last) {
-  T left = __shfl_up_sync(gm, last, 1, G);
+// One row step of a lane, in place: A holds row r - 1 of its C diagonals
+// (r = tau - g) and receives row r.  Cell (r, d) takes the minimum of
+// (r, d-1) (the cell to its left: A[c-1] already updated, or the left lane's
+// last cell of the previous step), (r-1, d) (A[c], not yet updated) and
+// (r-1, d+1) (A[c+1], or the right lane's first cell of this step), plus
+// (q[r] - t[r + d])^2; pen[c] is +inf for diagonals past the band.  qr is
+// q[r] and tw(c) returns t[r + d_lo + c].  With LIVE false the lane keeps its
+// row (a lane that has not reached row 0 yet), and its neighbours read its
+// unchanged cells: for row 0 those are the virtual row -1 (0 on d = 0, +inf
+// elsewhere), exactly what row 0 needs.
+template <typename T, int C, int G, typename TW>
+__device__ __forceinline__ void band_step(T qr, const TW& tw, bool live, int g, unsigned int gm,
+                                          T INF, const T (&pen)[C], T (&A)[C]) {
+  T left = __shfl_up_sync(gm, A[C - 1], 1, G);
   if (g == 0) left = INF;
-  const T qr = qg[tau];
-  const T* tp = tg + tau;
   {
-    const T d = qr - tp[0];
-    const T v = fmin3_(in[1 < C ? 1 : 0], in[0], left);
-    out[0] = fmax_(fma(d, d, v), pen[0]);
+    const T d = qr - tw(0);
+    const T v = fmin3_(A[1], A[0], left);
+    const T x = fmax_(fma(d, d, v), pen[0]);
+    A[0] = live ? x : A[0];
   }
-  T right = __shfl_down_sync(gm, out[0], 1, G);
+  T right = __shfl_down_sync(gm, A[0], 1, G);
   if (g == G - 1) right = INF;
 #pragma unroll
   for (int c = 1; c < C; ++c) {
-    const T up = (c + 1 < C) ? in[c + 1 < C ? c + 1 : 0] : right;
-    const T d = qr - tp[c];
-    const T v = fmin3_(up, in[c], out[c - 1]);
-    out[c] = fmax_(fma(d, d, v), pen[c]);
+    const T up = (c + 1 < C) ? A[c + 1 < C ? c + 1 : 0] : right;
+    const T d = qr - tw(c);
+    const T v = fmin3_(up, A[c], A[c - 1]);
+    const T x = fmax_(fma(d, d, v), pen[c]);
+    A[c] = live ? x : A[c];
   }
-  last = out[C - 1];
 }
 
 // Banded DTW of q (rows) against t (columns), squared cost.  A group of G
 // lanes computes one pair; lane g owns the C consecutive diagonals
 // d = -w + gC .. -w + gC + C - 1 and handles row tau - g at step tau.  The
-// first G steps (the lanes starting one after another) keep a lane's row
-// until it reaches row 0; after them two row buffers alternate, two steps per
-// iteration.  With ABANDON the group checks every 16 steps whether every
-// lane's latest row, plus the cumulative bound of the rows still ahead,
-// exceeds the threshold; it then returns +inf and reports the cells it swept.
+// first G steps (the lanes starting one after another) and the last few read
+// q and t from shared memory cell by cell.  In between the steps run in
+// blocks of C: a lane needs q[tau - g + k] and t[tau + k + x], k < C,
+// x < 2C - 1, over a block (its cells of consecutive steps overlap in t), so
+// it loads C values of q and C new values of t per block into registers and
+// keeps the C - 1 values of t the next block shares: two shared-memory loads
+// and two shuffles per step for C cells.  With ABANDON the group checks about
+// every 16 steps whether every lane's latest row, plus the cumulative bound
+// of the rows still ahead, exceeds the threshold; it then returns +inf and
+// reports the cells it swept.
 template <typename T, int C, int G, bool ABANDON>
 __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, int w,
                       const float* __restrict__ cbc, int nc, float thr,
                       const unsigned int* bsf2, unsigned int gm, int g,
                       unsigned long long* cells, bool* abandoned) {
+  static_assert(C >= 2, "a lane's first cell must not need its right neighbour's");
   const T INF = Pad<T>::inf();
   const int d_lo = -w + g * C;
-  T pen[C], A[C], B[C];
+  T pen[C], A[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) {
     pen[c] = (d_lo + c <= w) ? T(0) : INF;
@@ -145,22 +154,37 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
   const T* tg = t - g + d_lo;  // tg[tau + c] = t[row + d_lo + c]
   const int g0 = w / C, c0 = w % C;
   const int tau_end = m - 1 + g0;  // lane g0 (cell c0 on d = 0) reaches row m - 1
-  T last = INF;
   *abandoned = false;
   // warm-up: a lane that has not reached row 0 keeps its initial row
   const int warm = G < tau_end + 1 ? G : tau_end + 1;
-  for (int tau = 0; tau < warm; ++tau) {
-    band_step<T, C, G>(qg, tg, tau, g, gm, INF, pen, A, B, last);
-    const bool live = tau - g >= 0;
-#pragma unroll
-    for (int c = 0; c < C; ++c) A[c] = live ? B[c] : A[c];
+  int tau = 0;
+  for (; tau < warm; ++tau) {
+    const T* tp = tg + tau;
+    band_step<T, C, G>(qg[tau], [tp](int c) { return tp[c]; }, tau - g >= 0, g, gm, INF, pen, A);
   }
-  int tau = warm;
-  while (tau < tau_end) {  // two steps left at least
-    band_step<T, C, G>(qg, tg, tau, g, gm, INF, pen, A, B, last);
-    band_step<T, C, G>(qg, tg, tau + 1, g, gm, INF, pen, B, A, last);
-    tau += 2;
-    if (ABANDON && ((tau - warm) & 15) == 0 && tau <= tau_end) {
+  // blocks of C steps with q and t in registers
+  constexpr int kAbEvery = (16 + C - 1) / C;  // blocks between abandon checks
+  int ab_count = kAbEvery;
+  T W[2 * C - 1];  // W[x] = tg[tau + x] at the block's first step tau
+  if (tau + C - 1 <= tau_end) {
+#pragma unroll
+    for (int x = 0; x < C - 1; ++x) W[x] = tg[tau + x];
+  }
+  while (tau + C - 1 <= tau_end) {
+    T Qv[C];
+#pragma unroll
+    for (int x = 0; x < C; ++x) {
+      W[C - 1 + x] = tg[tau + C - 1 + x];
+      Qv[x] = qg[tau + x];
+    }
+#pragma unroll
+    for (int k = 0; k < C; ++k)
+      band_step<T, C, G>(Qv[k], [&W, k](int c) { return W[k + c]; }, true, g, gm, INF, pen, A);
+#pragma unroll
+    for (int x = 0; x < C - 1; ++x) W[x] = W[x + C];
+    tau += C;
+    if (ABANDON && --ab_count == 0 && tau <= tau_end) {
+      ab_count = kAbEvery;
       const int r = tau - 1 - g;  // this lane's latest row
       T fm = A[0];
 #pragma unroll
@@ -188,10 +212,10 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
       }
     }
   }
-  if (tau == tau_end) {  // an odd last step
-    band_step<T, C, G>(qg, tg, tau, g, gm, INF, pen, A, B, last);
-#pragma unroll
-    for (int c = 0; c < C; ++c) A[c] = B[c];
+  // the last steps (fewer than C)
+  for (; tau <= tau_end; ++tau) {
+    const T* tp = tg + tau;
+    band_step<T, C, G>(qg[tau], [tp](int c) { return tp[c]; }, true, g, gm, INF, pen, A);
   }
   T result = INF;
 #pragma unroll
@@ -263,26 +287,47 @@ __global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const i
       kl = __shfl_sync(gm, kl, 0, G);
       kr = __shfl_sync(gm, kr, 0, G);
       // ---- cumulative bound for abandoning: LB_Keogh terms of the rows (q)
-      // against the envelope of window j, in 8-row chunks, suffix-summed.
-      // Lane g owns chunks [g per, g per + per): it sums its block from the
-      // end, then adds the totals of the lanes above it (suffix scan). ----
+      // against the envelope of window j, summed over 8-row chunks, then
+      // suffix-summed over the chunks.  The group takes G consecutive rows
+      // at a time (coalesced envelope loads, conflict-free reads of q); the
+      // rows of a chunk sit in min(G, 8) consecutive lanes and are added by
+      // shuffles (two passes of four lanes when G = 4). ----
+      constexpr int kSeg = G < 8 ? G : 8;
+      float hold = 0.0f;
+      for (int k0 = 0; k0 < m; k0 += G) {
+        const int k = k0 + g;
+        float term = 0.0f;
+        if (k < m) {
+          if (k < kBias || k >= m - kBias) {
+            term = k == 0 ? kl : (k == m - kBias ? kr : 0.0f);
+          } else {
+            const float U = (float)((S.U[j + k] - mj) * sj), L = (float)((S.L[j + k] - mj) * sj);
+            const float d = fmaxf(fmaxf(q[k] - U, L - q[k]), 0.0f);
+            term = d * d;
+          }
+        }
+#pragma unroll
+        for (int o = 1; o < kSeg; o <<= 1) term += __shfl_xor_sync(gm, term, o, G);
+        if (kSeg == 8) {
+          if ((g & 7) == 0 && k < m) cbc[k >> 3] = term;
+        } else if (g == 0) {
+          if ((k0 & 4) == 0) {
+            hold = term;
+            if (k0 + 4 >= m) cbc[k0 >> 3] = hold;
+          } else {
+            cbc[k0 >> 3] = hold + term;
+          }
+        }
+      }
+      __syncwarp(gm);
+      // lane g owns chunks [g per, g per + per): it suffix-sums its own from
+      // the end, then adds the totals of the lanes above it
       const int per = (lay.nc + G - 1) / G;
       float run = 0.0f;
       for (int u = per - 1; u >= 0; --u) {
         const int x = g * per + u;
         if (x >= lay.nc) continue;
-        float acc = 0.0f;
-        const int k1 = 8 * x + 8 < m ? 8 * x + 8 : m;
-        for (int k = 8 * x; k < k1; ++k) {
-          if (k < kBias || k >= m - kBias) {
-            acc += k == 0 ? kl : (k == m - kBias ? kr : 0.0f);
-          } else {
-            const float U = (float)((S.U[j + k] - mj) * sj), L = (float)((S.L[j + k] - mj) * sj);
-            const float d = fmaxf(fmaxf(q[k] - U, L - q[k]), 0.0f);
-            acc = fmaf(d, d, acc);
-          }
-        }
-        run += acc;
+        run += cbc[x];
         cbc[x] = run;
       }
       float above = run;  // inclusive suffix scan of the lane totals
@@ -474,7 +519,8 @@ void run_list(const DevSeries& S, const int2* pairs, const Candidate* cands,
               const unsigned int* count_ptr, int count, const unsigned int* bsf2, double* out,
               cudaStream_t st) {
   const int pq = G + 1, pt = G * C + G + 2;
-  const int elems = ((2 * pq + 2 * pt + 2 * S.m) + 3) & ~3;
+  int elems = 2 * pq + 2 * pt + 2 * S.m;
+  elems += sizeof(T) == 4 ? ((17 - elems % 32) + 32) % 32 : ((9 - elems % 16) + 16) % 16;
   int threads = 128;
   size_t bytes = (size_t)(threads / G) * elems * sizeof(T);
   while (bytes > 100 * 1024 && threads > G && threads > 32) {
@@ -531,6 +577,21 @@ int band_shapes(int w, BandShape* out, int max) {
 
 bool choose_band(int w, BandShape* out) {
   const int cells = 2 * w + 1;
+  // One pair per warp (G = 32) when that leaves at most 40 % of the lanes'
+  // cells outside the band: the groups of a warp that hold different pairs
+  // leave the band loop at different steps (early abandoning), and the warp
+  // then runs their loops one after the other, which costs more than the
+  // wasted cells.  Otherwise the layout that wastes the fewest cells.
+  {
+    int C = (cells + 31) / 32;
+    if (C < 2) C = 2;
+    while (C <= 16 && !band_supported(C, 32)) ++C;
+    if (C <= 16 && 10 * (32 * C - cells) <= 4 * 32 * C) {
+      out->C = C;
+      out->G = 32;
+      return true;
+    }
+  }
   const int Gs[4] = {32, 16, 8, 4};
   double best = 2.0;
   BandShape pick = {0, 0};
@@ -653,7 +714,8 @@ template <typename T, int C, int G>
 void run_pairs64(const DevSeries& S, const int64_t* pi, const int64_t* pj, int64_t count,
                  double* out, cudaStream_t st) {
   const int pq = G + 1, pt = G * C + G + 2;
-  const int elems = ((2 * pq + 2 * pt + 2 * S.m) + 3) & ~3;
+  int elems = 2 * pq + 2 * pt + 2 * S.m;
+  elems += sizeof(T) == 4 ? ((17 - elems % 32) + 32) % 32 : ((9 - elems % 16) + 16) % 16;
   int threads = 128;
   size_t bytes = (size_t)(threads / G) * elems * sizeof(T);
   while (bytes > 100 * 1024 && threads > G && threads > 32) {
