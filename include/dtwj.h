@@ -257,7 +257,11 @@ int dtwj_ctx_set_exchange(dtwj_ctx* ctx, dtwj_exchange_fn fn, void* user, int32_
  * (returns how many; writes up to max); dtwj_time_band measures one of them
  * on exact FP32 DTW of `pairs` window pairs of a seeded random walk (band
  * cells per second); dtwj_ctx_set_band makes a context's joins use layout
- * (C, G) for band w (0, 0: back to the default choice). */
+ * (C, G) for band w (0, 0: back to the default choice).  The default for a
+ * join is G = 32 with the smallest C that covers the band (pairs abandon at
+ * different rows, and groups sharing a warp would then run one after the
+ * other); pair lists (dtwj_pair_dtw) take the layout wasting the fewest
+ * cells. */
 int dtwj_band_shapes(int32_t w, int32_t* C, int32_t* G, int32_t max);
 int dtwj_time_band(int device, int32_t m, int32_t w, int32_t C, int32_t G, int32_t pairs,
                    double* cells_per_s);

@@ -2,9 +2,11 @@
 
 The banded DTW runs G lanes per pair with C band cells per lane; every layout
 that covers the band computes the same distances, so the choice is only about
-speed.  `tune` times each candidate (band cells per second on exact FP32 DTW
-of random-walk window pairs, dtwj_time_band) and keeps the fastest; results
-are cached in a JSON file:
+speed.  `tune` times each candidate and keeps the fastest.  The default timer
+is band cells per second on exact FP32 DTW of random-walk window pairs
+(dtwj_time_band); `join_timer(sample)` times joins of a sample series instead,
+which includes early abandoning (groups that share a warp then fall out of
+step, which favours one pair per warp).  Results are cached in a JSON file:
 
     {"m=1024,w=52": {"C": 7, "G": 16, "cells_per_s": ..., "tried": [[C, G, cells_per_s], ...]}}
 
@@ -17,10 +19,25 @@ import os
 import sys
 
 if __package__:
-    from . import band_shapes, time_band
+    from . import PHASES, Context, F_PROFILE, band_shapes, time_band
 else:  # loaded by path
     _pkg = sys.modules.get("dtwj")
     band_shapes, time_band = _pkg.band_shapes, _pkg.time_band
+    Context, F_PROFILE, PHASES = _pkg.Context, _pkg.F_PROFILE, _pkg.PHASES
+
+
+def join_timer(series, device: int = 0):
+    """A timer for `tune` that joins `series` (a representative sample, e.g.
+    a prefix of the series to be joined) with each layout and returns the DTW
+    stage's band cells per second (`pairs` is ignored)."""
+    def timer(m, w, C, G, pairs):
+        with Context(device) as ctx:
+            ctx.set_band(min(w, m - 1), C, G)
+            ctx.join(series, m, w)  # warm-up (kernel loading, graph capture)
+            r = ctx.join(series, m, w, F_PROFILE)
+        t = r.phase_seconds[PHASES.index("pairs")]
+        return r.dtw_cells / t if t > 0 else float("inf")
+    return timer
 
 
 def _key(m: int, w: int) -> str:

@@ -223,9 +223,12 @@ struct BandShape {
   int C;  // cells (diagonals) per lane
   int G;  // lanes per pair
 };
-// Picks lanes-per-pair G in {4, 8, 16, 32} and cells-per-lane C in [2, 16]
-// covering 2w+1 diagonals with the least waste.  Returns false if w > 255.
+// The join's layout: one pair per warp (G = 32) with the fewest cells per
+// lane C in [2, 16] covering 2w+1 diagonals.  Returns false if w > 255.
 bool choose_band(int w, BandShape* out);
+// Exact DTW lists (no early abandoning): G in {4, 8, 16, 32} and C in
+// [2, 16] covering 2w+1 diagonals with the least waste.
+bool choose_band_list(int w, BandShape* out);
 // (C, G) has a kernel instantiation and covers band w.
 bool band_shape_ok(int w, int C, int G);
 // The shapes the autotuner tries for band w (per G the two smallest covering

@@ -1174,7 +1174,7 @@ int dtwj_pair_dtw(const double* x, int64_t n, int32_t m, int32_t w, const int64_
   if (count == 0) return DTWJ_OK;
   const int we = effective_band(m, w);
   BandShape band;
-  if (!choose_band(we, &band)) return DTWJ_ERR_BAND;
+  if (!choose_band_list(we, &band)) return DTWJ_ERR_BAND;
   dtwj_ctx* ctx = nullptr;
   rc = dtwj_ctx_create(0, &ctx);
   if (rc) return rc;

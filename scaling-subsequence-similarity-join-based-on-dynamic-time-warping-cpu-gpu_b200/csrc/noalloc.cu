@@ -57,7 +57,7 @@ extern "C" int dtwj_pair_dtw_noalloc(const double* x_dev, int64_t n, int32_t m, 
   if (count == 0) return DTWJ_OK;
   const int we = w > m - 1 ? m - 1 : w;
   BandShape band;
-  if (!choose_band(we, &band)) return DTWJ_ERR_BAND;
+  if (!choose_band_list(we, &band)) return DTWJ_ERR_BAND;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) {
     cudaGetLastError();

@@ -576,22 +576,27 @@ int band_shapes(int w, BandShape* out, int max) {
 }
 
 bool choose_band(int w, BandShape* out) {
+  // One pair per warp (G = 32), with the fewest cells per lane that cover
+  // the band.  The groups of a warp that hold different pairs leave the band
+  // loop at different steps (early abandoning) and the warp then runs their
+  // loops one after the other, which costs more than the lanes' cells
+  // outside the band: measured in joins of ECG-like series at w = 3, 13, 52
+  // and 103, G = 32 was fastest at every w, up to 4.9x ahead of the layout
+  // with the fewest wasted cells (w = 13: (7, 4) 58.9 s against (2, 32)
+  // 12.0 s of DTW).
+  int C = (2 * w + 1 + 31) / 32;
+  if (C < 2) C = 2;
+  while (C <= 16 && !band_supported(C, 32)) ++C;
+  if (C > 16) return false;
+  out->C = C;
+  out->G = 32;
+  return true;
+}
+
+bool choose_band_list(int w, BandShape* out) {
+  // Lists of exact DTWs run every pair to the end, so the groups of a warp
+  // stay in step: the layout that wastes the fewest cells.
   const int cells = 2 * w + 1;
-  // One pair per warp (G = 32) when that leaves at most 40 % of the lanes'
-  // cells outside the band: the groups of a warp that hold different pairs
-  // leave the band loop at different steps (early abandoning), and the warp
-  // then runs their loops one after the other, which costs more than the
-  // wasted cells.  Otherwise the layout that wastes the fewest cells.
-  {
-    int C = (cells + 31) / 32;
-    if (C < 2) C = 2;
-    while (C <= 16 && !band_supported(C, 32)) ++C;
-    if (C <= 16 && 10 * (32 * C - cells) <= 4 * 32 * C) {
-      out->C = C;
-      out->G = 32;
-      return true;
-    }
-  }
   const int Gs[4] = {32, 16, 8, 4};
   double best = 2.0;
   BandShape pick = {0, 0};

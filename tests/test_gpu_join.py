@@ -255,7 +255,7 @@ def test_every_band_layout_gives_the_same_join(gpu_dtwj, golden, synth, oracle):
                 _check(ctx.join(xs, m, w), i, j, d, (m, w, C, G))
 
 
-def test_autotune_measures_and_applies(gpu_dtwj, tmp_path):
+def test_autotune_measures_and_applies(gpu_dtwj, synth, tmp_path):
     import importlib.util
     spec = importlib.util.spec_from_file_location(
         "dtwj.autotune", os.path.join(PKG_DIR, "autotune.py"))
@@ -266,6 +266,10 @@ def test_autotune_measures_and_applies(gpu_dtwj, tmp_path):
         e = at.apply(ctx, 128, 6, path, pairs=512)
     assert e["cells_per_s"] > 0 and e["C"] * e["G"] >= 13
     assert all(t[2] > 0 for t in e["tried"])
+    # timed on joins of a sample series (early abandoning included)
+    e2 = at.tune(128, 6, None, timer=at.join_timer(synth.ecg_like(6000, 2)))
+    assert e2["cells_per_s"] > 0 and e2["C"] * e2["G"] >= 13
+    assert all(t[2] > 0 for t in e2["tried"])
 
 
 @pytest.mark.parametrize("world", [2, 3])
