@@ -3,6 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload NAME]
+    python bench.py --batch 4096     (the batched-join configuration, one line)
 
 Workload (default): one float64 random walk, n = 1,000,000, seed 1, with one
 planted motif pair (length-1024 sum of 3 sines, N(0, 0.1) noise, +-5 % time
@@ -503,6 +504,50 @@ def run_ours(args):
     return 0
 
 
+def run_batch(args):
+    """The batched-join configuration: args.batch series of uneven length
+    (log-uniform 2,000-65,536 samples), half random walks and half ECG-like,
+    m from {64, 128, 256}, ratio 0.05, each with its own top-1 pair.  Times
+    dtwj_join_batch (the series of one (m, w) joined together, one pass each)
+    against the same series joined one by one on one context, both from host
+    buffers (H2D inside the timed region), and checks that every series gets
+    the same pair and distance both ways."""
+    dtwj, synth = _load_pkg()
+    items = synth.batch_workload(count=args.batch)
+    xs = [it["series"] for it in items]
+    ms = [it["m"] for it in items]
+    ws = [it["w"] for it in items]
+    samples = int(sum(x.size for x in xs))
+    # warm-up: kernels loaded for every (m, w) group
+    warm = []
+    for mm in (64, 128, 256):
+        warm += [k for k in range(len(items)) if ms[k] == mm][:2]
+    dtwj.join_batch([xs[k] for k in warm], [ms[k] for k in warm], [ws[k] for k in warm])
+    t0 = time.perf_counter()
+    rb = dtwj.join_batch(xs, ms, ws)
+    t_batch = time.perf_counter() - t0
+    with dtwj.Context() as ctx:
+        for k in warm:
+            ctx.join(xs[k], ms[k], ws[k])
+        t0 = time.perf_counter()
+        r1 = [ctx.join(x, m, w) for x, m, w in zip(xs, ms, ws)]
+        t_one = time.perf_counter() - t0
+    same = all((a.i, a.j, a.dist) == (b.i, b.j, b.dist) for a, b in zip(rb, r1))
+    groups = sorted({(m, dtwj.band(m, 0.05)) for m in ms})
+    line = {
+        "metric": "batched join of %d series (config 4), series/s" % len(items),
+        "value": len(items) / t_batch, "unit": "series/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "higher_is_better": True, "dtype": "f64+f32", "data": "synthetic (seeded)",
+        "config": {"workload": "batch_workload(count=%d, seed=5)" % len(items),
+                   "samples": samples, "groups_m_w": groups},
+        "batch_seconds": t_batch, "one_by_one_seconds": t_one,
+        "speedup_vs_one_by_one": t_one / t_batch, "identical_per_series": same,
+        "timing": "host wall clock around the public API calls (series uploaded inside)",
+    }
+    print(json.dumps(line))
+    return 0 if same else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -515,7 +560,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--learned-reps", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="time the batched join of this many series (config 4) instead")
     args = ap.parse_args()
+    if args.batch > 0:
+        return run_batch(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

@@ -123,6 +123,12 @@ def workload(name: str):
         x = random_walk(4_000_000, 4)
         planted = plant_motifs(x, 8, 256, 4)
         return dict(series=x, m=256, w=band(256, 0.05), ratio=0.05, planted=planted)
+    if name == "rw4m_motif8_1m":  # the first 1,000,000 samples of rw4m_motif8
+        full = workload("rw4m_motif8")
+        n = 1_000_000
+        x = full["series"][:n].copy()
+        planted = [p for p in full["planted"] if max(p) + 256 <= n]
+        return dict(series=x, m=256, w=band(256, 0.05), ratio=0.05, planted=planted)
     raise KeyError(name)
 
 
