@@ -46,6 +46,27 @@ struct Timer {
   }
 };
 
+// What one chunk of the sweep left behind: whether one of its queues
+// overflowed (pairs were dropped, so the chunk is swept again), and the
+// counters after it, so that a chunk swept again can be taken out of them.
+struct ChunkNote {
+  unsigned long long counters[kNumCounters];
+  unsigned int overflow;
+  unsigned int pad;
+};
+
+// Runs after a chunk's last stage on the join's stream: notes the chunk and
+// clears the overflow bit for the next one.
+__global__ void k_chunk_note(int* status, const unsigned long long* counters, ChunkNote* note) {
+  const int t = threadIdx.x;
+  if (t < kNumCounters) note->counters[t] = counters[t];
+  if (t == 0) {
+    const int s = *status;
+    note->overflow = (s & 2) ? 1u : 0u;
+    *status = s & ~2;
+  }
+}
+
 }  // namespace
 
 struct dtwj_ctx {
@@ -82,7 +103,7 @@ enum BufId {
   B_BSF2, B_COUNTERS, B_CAND, B_CCOUNT, B_SEEDS, B_NSEEDS, B_VERIFY, B_BEST, B_PAIRS, B_OUT,
   B_MP, B_MPI, B_CB, B_AF, B_ULF, B_BITS, B_LBTILES, B_KQ, B_SBEG, B_SID, B_SEEDBSF,
   B_BEST_IJ, B_BEST_F32, B_QSER, B_TILEBEST, B_FEAT, B_SCORE, B_PA, B_CMAX, B_RW,
-  B_MPX_WANT, B_MPX_WREV, B_MPX_MIN, B_MPX_IDX, B_MPX_CAND, B_MPX_CNT,
+  B_MPX_WANT, B_MPX_WREV, B_MPX_MIN, B_MPX_IDX, B_MPX_CAND, B_MPX_CNT, B_NOTES, B_NOTES2,
   B_COUNT_
 };
 
@@ -523,43 +544,90 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
     launch_pairs(S, Q, Q.queue, Q.queue_count, true, band, ctx->num_sms, st);
     ph.end(DTWJ_PHASE_PAIRS, 1);
   };
-  // one pass over all tiles in chunks: bound sweep, run filter, LB_Keogh, DTW
-  auto sweep = [&](int ch) -> int {
-    for (int t0 = 0; t0 < nlb; t0 += ch) {
-      const int t1 = t0 + ch < nlb ? t0 + ch : nlb;
-      CUDA_OK(cudaMemsetAsync(qc, 0, 32, st));
-      ph.begin();
-      launch_lb(S, Q, lbtiles, t0, t1, bits, enumerate_all, lb_next, ctx->num_sms, st);
-      ph.end(DTWJ_PHASE_DIAG, 1);
-      filter_chunk(t0, t1);
-    }
+  // one pass over tile ranges: bound sweep, run filter, LB_Keogh, DTW, and a
+  // note of each range (queue overflow, counters after it); notes[0] holds
+  // the counters before the pass, notes[c + 1] those after range c
+  using Range = std::pair<int, int>;
+  auto sweep_range = [&](const Range& r, ChunkNote* note) {
+    CUDA_OK(cudaMemsetAsync(qc, 0, 32, st));
+    ph.begin();
+    launch_lb(S, Q, lbtiles, r.first, r.second, bits, enumerate_all, lb_next, ctx->num_sms, st);
+    ph.end(DTWJ_PHASE_DIAG, 1);
+    filter_chunk(r.first, r.second);
+    k_chunk_note<<<1, 32, 0, st>>>(S.status, Q.counters, note);
+    return DTWJ_OK;
+  };
+  auto sweep = [&](const std::vector<Range>& rg, ChunkNote* notes) -> int {
+    k_chunk_note<<<1, 32, 0, st>>>(S.status, Q.counters, notes);
+    for (size_t c = 0; c < rg.size(); ++c) sweep_range(rg[c], notes + c + 1);
     CUDA_OK(cudaGetLastError());
     return DTWJ_OK;
   };
+  std::vector<Range> ranges;
+  for (int t0 = 0; t0 < nlb; t0 += chunk) ranges.push_back({t0, t0 + chunk < nlb ? t0 + chunk : nlb});
+  ChunkNote* notes;
+  ENSURE(B_NOTES, (ranges.size() + 1) * sizeof(ChunkNote), notes);
   // a sharded join with an exchange sweeps its tiles in phases and lets the
   // caller lower the best-so-far between them (direct launches)
   const bool exchanging = ctx->exchange && ctx->shard_world > 1 && !tq;
   auto sweep_phased = [&]() -> int {
     const int P = ctx->exchange_phases;
+    k_chunk_note<<<1, 32, 0, st>>>(S.status, Q.counters, notes);
+    size_t c = 0;
     for (int ph_i = 0; ph_i < P; ++ph_i) {
-      const int a = (int)((int64_t)nlb * ph_i / P), b = (int)((int64_t)nlb * (ph_i + 1) / P);
-      for (int t0 = a; t0 < b; t0 += chunk) {
-        const int t1 = t0 + chunk < b ? t0 + chunk : b;
-        CUDA_OK(cudaMemsetAsync(qc, 0, 32, st));
-        ph.begin();
-        launch_lb(S, Q, lbtiles, t0, t1, bits, enumerate_all, lb_next, ctx->num_sms, st);
-        ph.end(DTWJ_PHASE_DIAG, 1);
-        filter_chunk(t0, t1);
-      }
+      const int b = (int)((int64_t)nlb * (ph_i + 1) / P);
+      for (; c < ranges.size() && ranges[c].second <= b; ++c)
+        sweep_range(ranges[c], notes + c + 1);
       ctx->exchange(ctx->exchange_user, Q.bsf2, nslots, (void*)st);
     }
+    for (; c < ranges.size(); ++c) sweep_range(ranges[c], notes + c + 1);
     CUDA_OK(cudaGetLastError());
     return DTWJ_OK;
   };
-  for (int attempt = 0;; ++attempt) {
+  // A batch sweeps chunk by chunk and checks each one: its short series put
+  // many tiles' survivors into one chunk, and when a chunk's queues
+  // overflow, the counters go back to before it, it is swept again in
+  // chunks an eighth its size, and the size grows back after chunks that
+  // fit, up to half the size that overflowed (a pass that is checked only at
+  // its end would sweep every overflowing chunk twice).
+  const bool adaptive = sbeg != nullptr && !exchanging && nlb > 0;
+  if (adaptive) {
+    ChunkNote* an;
+    ENSURE(B_NOTES2, 2 * sizeof(ChunkNote), an);
+    k_chunk_note<<<1, 32, 0, st>>>(S.status, Q.counters, an);
+    int ch = chunk, ch_max = chunk;
+    size_t resweeps = 0;
+    for (int t0 = 0; t0 < nlb;) {
+      const int t1 = t0 + ch < nlb ? t0 + ch : nlb;
+      sweep_range({t0, t1}, an + 1);
+      ChunkNote h[2];
+      CUDA_OK(cudaMemcpyAsync(h, an, sizeof h, cudaMemcpyDeviceToHost, st));
+      CUDA_OK(cudaStreamSynchronize(st));
+      if (!h[1].overflow) {
+        CUDA_OK(cudaMemcpyAsync(an, an + 1, sizeof(ChunkNote), cudaMemcpyDeviceToDevice, st));
+        t0 = t1;
+        ch = 2 * ch < ch_max ? 2 * ch : ch_max;
+        continue;
+      }
+      if (t1 - t0 == 1) return DTWJ_ERR_OVERFLOW;
+      ++resweeps;
+      CUDA_OK(cudaMemcpyAsync(Q.counters, h[0].counters, sizeof h[0].counters,
+                              cudaMemcpyHostToDevice, st));
+      CUDA_OK(cudaStreamSynchronize(st));  // h is read before it goes out of scope
+      ch_max = (t1 - t0) / 2 > 0 ? (t1 - t0) / 2 : 1;
+      ch = (t1 - t0) / 8 > 0 ? (t1 - t0) / 8 : 1;
+    }
+    CUDA_OK(cudaGetLastError());
+    if (verbose && resweeps)
+      fprintf(stderr, "dtwj: %zu chunks swept again in smaller chunks\n", resweeps);
+    ranges.clear();
+  }
+  for (int attempt = 0; !adaptive; ++attempt) {
     bool swept = false;
-    // only the first pass exchanges: a shard whose queues overflowed re-sweeps
-    // alone, and every shard must make the same exchange calls
+    ChunkNote* pass_notes = notes;
+    // only the first pass exchanges: a shard whose queues overflowed sweeps
+    // those chunks again alone, and every shard must make the same exchange
+    // calls
     if (exchanging && attempt == 0) {
       const int src = sweep_phased();
       if (src) return src;
@@ -574,9 +642,9 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
         key.insert(key.end(), b, b + bytes);
       };
       const int band_cg[2] = {band.C, band.G};
-      const int64_t misc[10] = {nlb, chunk, enumerate_all, masked, cascade, ctx->num_sms, ph.on,
+      const int64_t misc[11] = {nlb, chunk, enumerate_all, masked, cascade, ctx->num_sms, ph.on,
                                 (int64_t)ph.used, (int64_t)(uintptr_t)lbtiles,
-                                (int64_t)(uintptr_t)bits};
+                                (int64_t)(uintptr_t)bits, (int64_t)(uintptr_t)notes};
       put(&S, sizeof S);
       put(&Q, sizeof Q);
       put(band_cg, sizeof band_cg);
@@ -594,13 +662,13 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
         ctx->sweep_key.clear();
         const size_t u0 = ph.used, m0 = ph.marks.size();
         // events the capture records must exist before it starts
-        if (ph.on) ph.ev(u0 + 8 * ((size_t)(nlb + chunk - 1) / chunk) + 8);
+        if (ph.on) ph.ev(u0 + 8 * ranges.size() + 8);
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
         if (ok) {
           ph.capturing = true;
-          const int src = sweep(chunk);
+          const int src = sweep(ranges, notes);
           ph.capturing = false;
           ok = cudaStreamEndCapture(st, &graph) == cudaSuccess && src == DTWJ_OK && graph;
         }
@@ -628,18 +696,43 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
       }
     }
     if (!swept) {
-      const int src = sweep(chunk);
+      if (attempt > 0) {
+        // the chunks swept again get notes of their own (the first pass's
+        // buffer stays as the captured graph knows it)
+        ENSURE(B_NOTES2, (ranges.size() + 1) * sizeof(ChunkNote), pass_notes);
+      }
+      const int src = sweep(ranges, pass_notes);
       if (src) return src;
     }
-    // a survivor queue that overflowed loses pairs: sweep again in smaller chunks
-    int sweep_status = 0;
-    CUDA_OK(cudaMemcpyAsync(&sweep_status, S.status, 4, cudaMemcpyDeviceToHost, st));
+    // a chunk whose queue overflowed lost pairs: take its counts out and
+    // sweep it again in smaller chunks (the other chunks stand)
+    if (ranges.empty()) break;
+    std::vector<ChunkNote> nh(ranges.size() + 1);
+    CUDA_OK(cudaMemcpyAsync(nh.data(), pass_notes, nh.size() * sizeof(ChunkNote),
+                            cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
-    if (!(sweep_status & 2)) break;
-    if (chunk == 1 || attempt >= 4) return DTWJ_ERR_OVERFLOW;
-    chunk = chunk / 32 > 0 ? chunk / 32 : 1;
-    CUDA_OK(cudaMemsetAsync(S.status, 0, 4, st));
-    CUDA_OK(cudaMemsetAsync(Q.counters, 0, kNumCounters * 8, st));
+    std::vector<Range> again;
+    unsigned long long drop[kNumCounters] = {0};
+    size_t nbad = 0;
+    for (size_t c = 0; c < ranges.size(); ++c) {
+      if (!nh[c + 1].overflow) continue;
+      ++nbad;
+      for (int k = 0; k < kNumCounters; ++k)
+        drop[k] += nh[c + 1].counters[k] - nh[c].counters[k];
+      const int t0 = ranges[c].first, t1 = ranges[c].second;
+      if (t1 - t0 == 1 || attempt >= 4) return DTWJ_ERR_OVERFLOW;
+      const int sub = (t1 - t0) / 32 > 0 ? (t1 - t0) / 32 : 1;
+      for (int u = t0; u < t1; u += sub) again.push_back({u, u + sub < t1 ? u + sub : t1});
+    }
+    if (again.empty()) break;
+    if (verbose)
+      fprintf(stderr, "dtwj: queue overflow in %zu of %zu chunks, sweeping them again in %zu\n",
+              nbad, ranges.size(), again.size());
+    unsigned long long kept[kNumCounters];
+    for (int k = 0; k < kNumCounters; ++k) kept[k] = nh.back().counters[k] - drop[k];
+    CUDA_OK(cudaMemcpyAsync(Q.counters, kept, sizeof kept, cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaStreamSynchronize(st));  // kept is read before it goes out of scope
+    ranges.swap(again);
   }
 
   // ---- FP64 verification of the candidates, per-series minimum ----

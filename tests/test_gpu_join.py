@@ -343,3 +343,34 @@ def test_cli_reads_the_reference_file_formats(tmp_path, golden):
         out = subprocess.run([cli, str(data), str(tf), "256", "0.01"] + extra, capture_output=True,
                              text=True, check=True).stdout
         assert "first min is %d sec min is %d" % (c["i"] + 1, c["j"] + 1) in out, extra
+
+
+def test_queue_overflow_sweeps_only_the_chunks_again(gpu_dtwj, synth):
+    # With a small DTW queue (DTWJ_QUEUE_CAP, 2^20 pairs; LB_Keogh queue
+    # twice that) most pairs of the ECG-like 16k prefix reach DTW, so chunks
+    # overflow; each such chunk is swept again in smaller chunks, its counts
+    # taken out first.  The result equals the full-queue join and the oracle
+    # record, and every pair is counted once: the stage counters add up to
+    # the pair count plus at most the seed DTWs (700 slots).
+    import json
+    from conftest import GOLDEN
+    wl = synth.workload("ecg16k_w52")
+    x, m, w = wl["series"], wl["m"], wl["w"]
+    rec = {r["workload"]: r for r in json.load(open(os.path.join(GOLDEN, "fullsize.json")))}
+    rec = rec["ecg16k_w52"]
+    with gpu_dtwj.Context() as ctx:
+        full = ctx.join(x, m, w)
+    os.environ["DTWJ_QUEUE_CAP"] = str(1 << 20)
+    try:
+        with gpu_dtwj.Context() as ctx:
+            small = ctx.join(x, m, w)
+    finally:
+        del os.environ["DTWJ_QUEUE_CAP"]
+    assert (small.i, small.j, small.dist) == (full.i, full.j, full.dist)
+    assert (small.i, small.j) == (rec["i"], rec["j"])
+    assert abs(small.dist - rec["dist"]) <= 1e-5 * rec["dist"]
+    s = x.size - m + 1
+    for r in (full, small):
+        assert r.pairs == (s - m) * (s - m + 1) // 2
+        total = r.pruned_fast + r.pruned_paa + r.pruned_kim + r.pruned_keogh + r.dtw_calls
+        assert 0 <= total - r.pairs <= 700, (total, r.pairs)
