@@ -103,16 +103,19 @@ __host__ __device__ inline GroupLayout group_layout(int m, int w, int C, int G, 
 template <typename T, int C, int G, typename TW>
 __device__ __forceinline__ void band_step(T qr, const TW& tw, bool live, int g, unsigned int gm,
                                           T INF, const T (&pen)[C], T (&A)[C]) {
-  T left = __shfl_up_sync(gm, A[C - 1], 1, G);
-  if (g == 0) left = INF;
+  // Lane 0's left neighbour and lane G-1's right neighbour wrap around the
+  // group, so no lane needs a select: C G is even and 2w + 1 odd, so C G >
+  // 2w + 1 and lane G-1's last cell lies past the band; its +inf penalty
+  // keeps it +inf, which is what lane 0's first cell (d = -w) needs on its
+  // left, and makes whatever comes from the right irrelevant to it.
+  const T left = __shfl_sync(gm, A[C - 1], (g + G - 1) & (G - 1), G);
   {
     const T d = qr - tw(0);
     const T v = fmin3_(A[1], A[0], left);
     const T x = fmax_(fma(d, d, v), pen[0]);
     A[0] = live ? x : A[0];
   }
-  T right = __shfl_down_sync(gm, A[0], 1, G);
-  if (g == G - 1) right = INF;
+  const T right = __shfl_sync(gm, A[0], (g + 1) & (G - 1), G);
 #pragma unroll
   for (int c = 1; c < C; ++c) {
     const T up = (c + 1 < C) ? A[c + 1 < C ? c + 1 : 0] : right;
