@@ -378,20 +378,23 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 3) k_paa_lags(DevSeries S, Dev
 #pragma unroll 1
       for (int r4 = 0; r4 < 4; ++r4) {
         int k = r4;
-        for (; k + 12 < nb; k += 16) {
+        // block k's means at qi[0], qj[0]; the group's four at immediate offsets
+        const float4* qi = pi + r4 * B;
+        const float4* qj = pj + r4 * B;
+        for (; k + 12 < nb; k += 16, qi += 16 * B, qj += 16 * B) {
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             const int kk = k + 4 * u;
             const float o = kk < k_lo ? o_lo : (kk < k_hi ? o_mid : o_hi);
-            block_terms(pi[kk * B], pj[kk * B], fsi, fsj, o, acc1, acc2);
+            block_terms(qi[4 * u * B], qj[4 * u * B], fsi, fsj, o, acc1, acc2);
           }
           pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
           if (__all_sync(0xffffffffu, pruned)) break;
         }
         if (k + 12 < nb) break;  // every lane pruned
-        for (; k < nb; k += 4) {
+        for (; k < nb; k += 4, qi += 4 * B, qj += 4 * B) {
           const float o = k < k_lo ? o_lo : (k < k_hi ? o_mid : o_hi);
-          block_terms(pi[k * B], pj[k * B], fsi, fsj, o, acc1, acc2);
+          block_terms(qi[0], qj[0], fsi, fsj, o, acc1, acc2);
         }
         pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
         if (__all_sync(0xffffffffu, pruned)) break;

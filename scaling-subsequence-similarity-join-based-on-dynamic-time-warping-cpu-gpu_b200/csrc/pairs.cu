@@ -173,13 +173,17 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
 #pragma unroll
     for (int x = 0; x < C - 1; ++x) W[x] = tg[tau + x];
   }
+  const T* tb = tg + tau + C - 1;  // the block's new values of t, and of q,
+  const T* qb = qg + tau;           // at immediate offsets from two pointers
   while (tau + C - 1 <= tau_end) {
     T Qv[C];
 #pragma unroll
     for (int x = 0; x < C; ++x) {
-      W[C - 1 + x] = tg[tau + C - 1 + x];
-      Qv[x] = qg[tau + x];
+      W[C - 1 + x] = tb[x];
+      Qv[x] = qb[x];
     }
+    tb += C;
+    qb += C;
 #pragma unroll
     for (int k = 0; k < C; ++k)
       band_step<T, C, G>(Qv[k], [&W, k](int c) { return W[k + c]; }, true, g, gm, INF, pen, A);
