@@ -1,11 +1,11 @@
 // Tile-scoring MLP of the learned ordering: 64 -> 128 -> 128 -> 1 with ReLU,
 // mean squared error, Adam.  No counterpart in the reference.
 //
-// Every layer is a GEMM on the tensor cores: BF16 operands through
-// mma.sync.m16n8k16 (row x col, FP32 accumulation), FP32 activations and FP32
-// master weights; the BF16 copies of W1 and W2 are refreshed after every Adam
-// step.  A SIMT FP32 GEMM with the same interface is the debug path the
-// gradient check compares against (`precise`).
+// Every layer is a GEMM on the 5th-generation tensor cores (tcgen05.mma,
+// BF16 operands staged in shared memory, FP32 accumulator in tensor memory),
+// FP32 activations and FP32 master weights; the BF16 copies of W1 and W2 are
+// refreshed after every Adam step.  A SIMT FP32 GEMM with the same interface
+// is the debug path the gradient check compares against (`precise`).
 //
 // Parameter layout (FP32, 24,961 values): W1 [128][64], b1 [128],
 // W2 [128][128], b2 [128], w3 [128], b3 [1].
@@ -46,51 +46,176 @@ unsigned grid_for(int64_t n, int t = kThreads) {
 
 // ---- GEMM: C[m][n] (+)= sum_k A(m, k) B(k, n) ----
 // A(m, k) = A[m * sam + k * sak], B(k, n) = B[k * sbk + n * sbn], C row-major
-// with leading dimension ldc.  One warp per 16 x 8 output tile.
+// with leading dimension ldc.
+//
+// BF16 path on the 5th-generation tensor cores: a CTA of 4 warps computes
+// 128 rows x N columns (N <= 128, a multiple of 16) in a tensor-memory
+// accumulator.  K runs in stages of 64: the 4 warps stage the A and B tiles
+// (B transposed, both K-major) in shared memory in the canonical layout
+// without swizzle (8-row x 16-byte core matrices; the two core matrices of a
+// K-step of 16 are 128 bytes apart, 8-row groups 1024 bytes apart), one
+// thread issues the stage's four tcgen05.mma (M = 128, K = 16 each) and
+// commits them to an mbarrier, which every thread waits on before the next
+// stage overwrites the tiles.  Each warp then reads its 32 rows of the
+// accumulator (tcgen05.ld) and writes them to C.  The MLP's operands have
+// arbitrary strides (transposed operands in the weight gradients), so the
+// tiles are staged with ordinary loads rather than tensor-map copies.
 
 __device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
   const uint32_t l = __bfloat16_as_ushort(lo), h = __bfloat16_as_ushort(hi);
   return l | (h << 16);
 }
 
-__global__ void k_gemm_bf16(int M, int N, int K, const bf16* __restrict__ A, int64_t sam,
-                            int64_t sak, const bf16* __restrict__ B, int64_t sbk, int64_t sbn,
-                            float* __restrict__ C, int64_t ldc, bool accumulate) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int tn_count = (N + 7) / 8;
-  const int64_t tiles = (int64_t)((M + 15) / 16) * tn_count;
-  if (warp >= tiles) return;
-  const int tm = (int)(warp / tn_count), tn = (int)(warp % tn_count);
-  const int g = lane >> 2, tg = lane & 3;
-  const int r0 = tm * 16 + g, r1 = r0 + 8, nb = tn * 8 + g;
-  const bf16 z = __float2bfloat16(0.0f);
-  auto a_at = [&](int r, int k) { return (r < M && k < K) ? A[r * sam + k * sak] : z; };
-  auto b_at = [&](int k, int n) { return (k < K && n < N) ? B[k * sbk + n * sbn] : z; };
-  float d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
-  for (int k0 = 0; k0 < K; k0 += 16) {
-    const int c0 = k0 + tg * 2;
-    const uint32_t a0 = pack2(a_at(r0, c0), a_at(r0, c0 + 1));
-    const uint32_t a1 = pack2(a_at(r1, c0), a_at(r1, c0 + 1));
-    const uint32_t a2 = pack2(a_at(r0, c0 + 8), a_at(r0, c0 + 9));
-    const uint32_t a3 = pack2(a_at(r1, c0 + 8), a_at(r1, c0 + 9));
-    const uint32_t b0 = pack2(b_at(c0, nb), b_at(c0 + 1, nb));
-    const uint32_t b1 = pack2(b_at(c0 + 8, nb), b_at(c0 + 9, nb));
+constexpr int kTcRows = 128;   // rows of A (and of the accumulator) per CTA
+constexpr int kTcK = 64;       // K per stage
+constexpr int kTcCols = 128;   // accumulator columns allocated (N <= 128)
+constexpr uint32_t kTcLbo = 128, kTcSbo = 1024;  // canonical K-major strides, bytes
+constexpr int kTcWaitLimit = 1 << 24;            // mbarrier polls before giving up
+
+struct TcSmem {
+  alignas(1024) bf16 a[kTcRows * kTcK];
+  alignas(1024) bf16 b[kTcCols * kTcK];
+  alignas(8) uint64_t mbar;
+  uint32_t tmem;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Byte offset of element (r, k) of a K-major tile of kTcK columns.
+__device__ __forceinline__ uint32_t tc_offset(int r, int k) {
+  return (uint32_t)((r & 7) * 16 + (r >> 3) * kTcSbo + (k & 7) * 2 + (k >> 3) * kTcLbo);
+}
+
+// Shared-memory matrix descriptor: start address, leading (K) and stride
+// (8-row group) byte offsets in 16-byte units, descriptor version 1, no
+// swizzle.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((kTcLbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((kTcSbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t tc_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+// Polls the mbarrier for `phase`; false if it did not complete within the limit.
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t phase) {
+  for (int it = 0; it < kTcWaitLimit; ++it) {
+    uint32_t done;
     asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-        "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
-        : "+f"(d0), "+f"(d1), "+f"(d2), "+f"(d3)
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done) : "r"(mbar), "r"(phase) : "memory");
+    if (done) return true;
   }
-  const int n0 = tn * 8 + tg * 2;
-  const float v[4] = {d0, d1, d2, d3};
+  return false;
+}
+
+// Reads 32 accumulator columns of this warp's 32 lanes (one row per thread).
+__device__ __forceinline__ void tc_load32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Stages 128 (or N) rows x kTcK columns of op(r, k) into a K-major tile.
+template <typename Get>
+__device__ __forceinline__ void tc_stage(unsigned char* tile, int rows, int tid, const Get& get) {
+  for (int it = tid; it < rows * (kTcK / 8); it += 128) {
+    const int r = it / (kTcK / 8), kg = it % (kTcK / 8);
+    uint32_t v[4];
 #pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    const int r = e < 2 ? r0 : r1, n = n0 + (e & 1);
-    if (r < M && n < N) {
-      float* c = C + r * ldc + n;
-      *c = accumulate ? *c + v[e] : v[e];
+    for (int h = 0; h < 4; ++h) v[h] = pack2(get(r, kg * 8 + 2 * h), get(r, kg * 8 + 2 * h + 1));
+    *reinterpret_cast<uint4*>(tile + tc_offset(r, kg * 8)) = make_uint4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const bf16* __restrict__ A,
+                                                 int64_t sam, int64_t sak,
+                                                 const bf16* __restrict__ B, int64_t sbk,
+                                                 int64_t sbn, float* __restrict__ C, int64_t ldc,
+                                                 bool accumulate, int* status) {
+  extern __shared__ unsigned char tc_raw[];
+  TcSmem& sh = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) &
+                                          ~static_cast<uintptr_t>(1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kTcRows;
+  const uint32_t a_base = smem_u32(sh.a), b_base = smem_u32(sh.b), mbar = smem_u32(&sh.mbar);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&sh.tmem)), "r"(kTcCols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = sh.tmem;
+  const uint32_t idesc = tc_idesc(kTcRows, N);
+  const bf16 z = __float2bfloat16(0.0f);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int k0 = 0; k0 < K && ok; k0 += kTcK) {
+    tc_stage(reinterpret_cast<unsigned char*>(sh.a), kTcRows, tid, [&](int r, int k) {
+      const int m = m0 + r, kk = k0 + k;
+      return (m < M && kk < K) ? A[m * sam + kk * sak] : z;
+    });
+    tc_stage(reinterpret_cast<unsigned char*>(sh.b), N, tid, [&](int n, int k) {
+      const int kk = k0 + k;
+      return kk < K ? B[kk * sbk + n * sbn] : z;
+    });
+    // the tiles written by ordinary stores become visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int s = 0; s < kTcK / 16; ++s) {
+        const uint64_t ad = tc_desc(a_base + s * 2 * kTcLbo), bd = tc_desc(b_base + s * 2 * kTcLbo);
+        const uint32_t acc = (k0 > 0 || s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+            :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(mbar) : "memory");
     }
+    // the stage's products are in the accumulator and its tiles free again
+    ok = __syncthreads_and(tc_wait(mbar, phase)) != 0;
+    phase ^= 1u;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const int row = m0 + warp * 32 + lane;
+  for (int c0 = 0; c0 < N; c0 += 32) {
+    uint32_t v[32];
+    if (ok) tc_load32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    if (row < M) {
+      float* c = C + row * ldc + c0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const float x = ok ? __uint_as_float(v[j]) : __int_as_float(0x7fc00000);
+        c[j] = accumulate ? c[j] + x : x;
+      }
+    }
+  }
+  if (!ok && tid == 0) atomicOr(status, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                 :: "r"(tmem), "r"(kTcCols) : "memory");
   }
 }
 
@@ -219,6 +344,7 @@ struct dtwj_mlp {
   float *X = nullptr, *T = nullptr, *H1 = nullptr, *H2 = nullptr, *Y = nullptr, *DY = nullptr,
         *DH1 = nullptr, *DH2 = nullptr, *loss = nullptr;
   bf16 *Xb = nullptr, *H1b = nullptr, *DH1b = nullptr, *DH2b = nullptr;
+  int* tc_status = nullptr;  // set when a tensor-core GEMM gave up waiting on its mbarrier
 };
 
 namespace {
@@ -228,16 +354,19 @@ bool dalloc(T** p, int64_t count) {
   return cudaMalloc((void**)p, (size_t)count * sizeof(T)) == cudaSuccess;
 }
 
+// The BF16 path needs N <= 128 and N % 16 == 0 (the MLP's N are 64 and 128).
+constexpr int kTcSmemBytes = 48 * 1024;  // also keeps at most 4 CTAs (512 TMEM columns) per SM
+static_assert(sizeof(TcSmem) + 1024 <= kTcSmemBytes, "tcgen05 GEMM tiles");
+
 void gemm(bool precise, int M, int N, int K, const void* A, int64_t sam, int64_t sak,
           const void* B, int64_t sbk, int64_t sbn, float* C, int64_t ldc, bool acc,
-          cudaStream_t st) {
+          int* status, cudaStream_t st) {
   if (precise) {
     k_gemm_f32<<<grid_for((int64_t)M * N), kThreads, 0, st>>>(
         M, N, K, (const float*)A, sam, sak, (const float*)B, sbk, sbn, C, ldc, acc);
   } else {
-    const int64_t warps = (int64_t)((M + 15) / 16) * ((N + 7) / 8);
-    k_gemm_bf16<<<(unsigned)((warps * 32 + 127) / 128), 128, 0, st>>>(
-        M, N, K, (const bf16*)A, sam, sak, (const bf16*)B, sbk, sbn, C, ldc, acc);
+    k_gemm_tc<<<(unsigned)((M + kTcRows - 1) / kTcRows), 128, kTcSmemBytes, st>>>(
+        M, N, K, (const bf16*)A, sam, sak, (const bf16*)B, sbk, sbn, C, ldc, acc, status);
   }
 }
 
@@ -251,12 +380,12 @@ void pass(dtwj_mlp* net, int rows, bool train, bool precise) {
   // H1 = relu(X W1^T + b1): A = X [rows][64], B(k, n) = W1[n][k]
   if (!precise) k_to_bf16<<<grid_for((int64_t)rows * kIn), kThreads, 0, st>>>(net->X, net->Xb, (int64_t)rows * kIn);
   gemm(precise, rows, kHid, kIn, precise ? (const void*)net->X : net->Xb, kIn, 1,
-       precise ? (const void*)(P + kOffW1) : net->W1b, 1, kIn, net->H1, kHid, false, st);
+       precise ? (const void*)(P + kOffW1) : net->W1b, 1, kIn, net->H1, kHid, false, net->tc_status, st);
   k_bias_relu<<<gr, kThreads, 0, st>>>(net->H1, P + kOffB1, rows, kHid);
   // H2 = relu(H1 W2^T + b2)
   if (!precise) k_to_bf16<<<gr, kThreads, 0, st>>>(net->H1, net->H1b, (int64_t)rows * kHid);
   gemm(precise, rows, kHid, kHid, precise ? (const void*)net->H1 : net->H1b, kHid, 1,
-       precise ? (const void*)(P + kOffW2) : net->W2b, 1, kHid, net->H2, kHid, false, st);
+       precise ? (const void*)(P + kOffW2) : net->W2b, 1, kHid, net->H2, kHid, false, net->tc_status, st);
   k_bias_relu<<<gr, kThreads, 0, st>>>(net->H2, P + kOffB2, rows, kHid);
   if (train) cudaMemsetAsync(net->loss, 0, 4, st);
   k_head<<<grid_for((int64_t)rows * 32), kThreads, 0, st>>>(net->H2, P + kOffW3, P + kOffB3, rows,
@@ -271,17 +400,25 @@ void pass(dtwj_mlp* net, int rows, bool train, bool precise) {
   k_dh2<<<gr, kThreads, 0, st>>>(net->DY, P + kOffW3, net->H2, net->DH2, rows);
   if (!precise) k_to_bf16<<<gr, kThreads, 0, st>>>(net->DH2, net->DH2b, (int64_t)rows * kHid);
   gemm(precise, kHid, kHid, rows, precise ? (const void*)net->DH2 : net->DH2b, 1, kHid,
-       precise ? (const void*)net->H1 : net->H1b, kHid, 1, G + kOffW2, kHid, false, st);
+       precise ? (const void*)net->H1 : net->H1b, kHid, 1, G + kOffW2, kHid, false, net->tc_status, st);
   k_colsum<<<1, kHid, 0, st>>>(net->DH2, nullptr, rows, kHid, G + kOffB2);
   // dH1 = dH2 W2 . [H1 > 0]: A = dH2 [rows][128], B(k, n) = W2[k][n]
   gemm(precise, rows, kHid, kHid, precise ? (const void*)net->DH2 : net->DH2b, kHid, 1,
-       precise ? (const void*)(P + kOffW2) : net->W2b, kHid, 1, net->DH1, kHid, false, st);
+       precise ? (const void*)(P + kOffW2) : net->W2b, kHid, 1, net->DH1, kHid, false, net->tc_status, st);
   k_relu_grad<<<gr, kThreads, 0, st>>>(net->DH1, net->H1, (int64_t)rows * kHid);
   // dW1 = dH1^T X [128][64] (K = rows), db1
   if (!precise) k_to_bf16<<<gr, kThreads, 0, st>>>(net->DH1, net->DH1b, (int64_t)rows * kHid);
   gemm(precise, kHid, kIn, rows, precise ? (const void*)net->DH1 : net->DH1b, 1, kHid,
-       precise ? (const void*)net->X : net->Xb, kIn, 1, G + kOffW1, kIn, false, st);
+       precise ? (const void*)net->X : net->Xb, kIn, 1, G + kOffW1, kIn, false, net->tc_status, st);
   k_colsum<<<1, kHid, 0, st>>>(net->DH1, nullptr, rows, kHid, G + kOffB1);
+}
+
+// After the stream is synchronised: DTWJ_ERR_CUDA if a tensor-core GEMM gave
+// up waiting for its products (its outputs are NaN then).
+int tc_check(dtwj_mlp* net) {
+  int st = 0;
+  if (cudaMemcpy(&st, net->tc_status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return DTWJ_ERR_CUDA;
+  return st ? DTWJ_ERR_CUDA : DTWJ_OK;
 }
 
 void refresh_bf16(dtwj_mlp* net) {
@@ -329,7 +466,8 @@ int dtwj_mlp_create(int device, uint64_t seed, dtwj_mlp** out) {
             dalloc(&net->H2, B * kHid) && dalloc(&net->Y, B) && dalloc(&net->DY, B) &&
             dalloc(&net->DH1, B * kHid) && dalloc(&net->DH2, B * kHid) &&
             dalloc(&net->loss, 1) && dalloc(&net->Xb, B * kIn) && dalloc(&net->H1b, B * kHid) &&
-            dalloc(&net->DH1b, B * kHid) && dalloc(&net->DH2b, B * kHid);
+            dalloc(&net->DH1b, B * kHid) && dalloc(&net->DH2b, B * kHid) &&
+            dalloc(&net->tc_status, 1) && cudaMemset(net->tc_status, 0, 4) == cudaSuccess;
   if (!ok) {
     dtwj_mlp_destroy(net);
     return DTWJ_ERR_OOM;
@@ -351,7 +489,7 @@ void dtwj_mlp_destroy(dtwj_mlp* net) {
   if (net->stream) cudaStreamSynchronize(net->stream);
   void* bufs[] = {net->P,  net->G,  net->M1, net->M2,  net->W1b, net->W2b, net->X,
                   net->T,  net->H1, net->H2, net->Y,   net->DY,  net->DH1, net->DH2,
-                  net->loss, net->Xb, net->H1b, net->DH1b, net->DH2b};
+                  net->loss, net->Xb, net->H1b, net->DH1b, net->DH2b, net->tc_status};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (net->stream) cudaStreamDestroy(net->stream);
@@ -396,7 +534,7 @@ int dtwj_mlp_grad(dtwj_mlp* net, const float* x, const float* y, int64_t count, 
       cudaStreamSynchronize(net->stream) != cudaSuccess)
     return DTWJ_ERR_CUDA;
   if (loss) *loss = l;
-  return DTWJ_OK;
+  return tc_check(net);
 }
 
 int dtwj_mlp_train(dtwj_mlp* net, const float* x, const float* y, int64_t count, int32_t epochs,
@@ -443,7 +581,7 @@ int dtwj_mlp_train(dtwj_mlp* net, const float* x, const float* y, int64_t count,
     epoch_loss /= (double)seen;
   }
   if (last_loss) *last_loss = (float)epoch_loss;
-  return cudaGetLastError() == cudaSuccess ? DTWJ_OK : DTWJ_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? tc_check(net) : DTWJ_ERR_CUDA;
 }
 
 int dtwj_mlp_predict(dtwj_mlp* net, const float* x, int64_t count, float* out) {
@@ -458,7 +596,7 @@ int dtwj_mlp_predict(dtwj_mlp* net, const float* x, int64_t count, float* out) {
                         net->stream) != cudaSuccess)
       return DTWJ_ERR_CUDA;
   }
-  return cudaStreamSynchronize(net->stream) == cudaSuccess ? DTWJ_OK : DTWJ_ERR_CUDA;
+  return cudaStreamSynchronize(net->stream) == cudaSuccess ? tc_check(net) : DTWJ_ERR_CUDA;
 }
 
 int dtwj_mlp_save(dtwj_mlp* net, const char* path) {
@@ -514,7 +652,7 @@ int mlp_predict_device(dtwj_mlp* net, const float* x_dev, int64_t count, float* 
                         net->stream) != cudaSuccess)
       return DTWJ_ERR_CUDA;
   }
-  return cudaStreamSynchronize(net->stream) == cudaSuccess ? DTWJ_OK : DTWJ_ERR_CUDA;
+  return cudaStreamSynchronize(net->stream) == cudaSuccess ? tc_check(net) : DTWJ_ERR_CUDA;
 }
 
 int mlp_device(const dtwj_mlp* net) { return net->device; }
