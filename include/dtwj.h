@@ -266,6 +266,12 @@ int dtwj_band_shapes(int32_t w, int32_t* C, int32_t* G, int32_t max);
 int dtwj_time_band(int device, int32_t m, int32_t w, int32_t C, int32_t G, int32_t pairs,
                    double* cells_per_s);
 int dtwj_ctx_set_band(dtwj_ctx* ctx, int32_t w, int32_t C, int32_t G);
+/* Further tunables of a context's joins (no counterpart in the reference):
+ * the CTA size of the DTW kernel in warps (1, 2, 4 or 8; each warp is one
+ * pair in the default layout) and the tiles per chunk of the diagonal sweep
+ * (16 to 4096; a chunk's survivors share the queues).  0 restores a default
+ * (4 warps, 1024 tiles).  The result never depends on them. */
+int dtwj_ctx_set_tuning(dtwj_ctx* ctx, int32_t dtw_warps, int32_t chunk_tiles);
 
 /* Series files in the formats of the reference's loaders
  * (CPU_version1/loadfile.cpp:14-142, GPU_version1/src/loadfile.cu:13-148):

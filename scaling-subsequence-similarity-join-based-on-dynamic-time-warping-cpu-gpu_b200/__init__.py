@@ -76,6 +76,7 @@ EXPORTS = (
     "dtwj_band_shapes",
     "dtwj_time_band",
     "dtwj_ctx_set_band",
+    "dtwj_ctx_set_tuning",
     "dtwj_ctx_set_shard",
     "dtwj_ctx_set_exchange",
     "dtwj_load",
@@ -203,6 +204,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dtwj_band_shapes.argtypes = [i32, P(i32), P(i32), i32]
     lib.dtwj_time_band.argtypes = [ctypes.c_int, i32, i32, i32, i32, i32, P(d)]
     lib.dtwj_ctx_set_band.argtypes = [vp, i32, i32, i32]
+    lib.dtwj_ctx_set_tuning.argtypes = [vp, i32, i32]
     lib.dtwj_ctx_set_shard.argtypes = [vp, i32, i32]
     lib.dtwj_ctx_set_exchange.argtypes = [vp, EXCHANGE_FN, vp, i32]
     lib.dtwj_load.argtypes = [ctypes.c_char_p, ctypes.c_char_p, i32, i32, P(d), i64, P(i64)]
@@ -291,15 +293,31 @@ def make_exchange(group=None, device: int | None = None):
 
 
 class Context:
-    """Reusable device context (keeps device buffers between joins)."""
+    """Reusable device context (keeps device buffers between joins).
 
-    def __init__(self, device: int = 0):
+    tune_cache: a JSON file written by autotune.tune_join (default: the
+    DTWJ_TUNE_CACHE environment variable, if set).  Before the first join of
+    an (m, w) the context applies that file's entry for it, if there is one;
+    it never tunes by itself."""
+
+    def __init__(self, device: int = 0, tune_cache: str | None = None):
         lib = load()
         h = ctypes.c_void_p()
         rc = lib.dtwj_ctx_create(device, ctypes.byref(h))
         if rc != OK:
             raise DtwjError(rc, "dtwj_ctx_create")
         self._h = h
+        self._tune_cache = tune_cache if tune_cache is not None else os.environ.get("DTWJ_TUNE_CACHE")
+        self._tuned = set()
+
+    def _apply_tuning(self, m: int, w: int):
+        if not self._tune_cache or (m, w) in self._tuned:
+            return
+        self._tuned.add((m, w))
+        from . import autotune
+        e = autotune.load_cache(self._tune_cache).get(autotune.join_key(m, w))
+        if e:
+            autotune.apply_entry(self, m, w, e)
 
     def close(self):
         if self._h:
@@ -319,6 +337,7 @@ class Context:
             pass
 
     def join(self, x, m: int, w: int, flags: int = 0) -> JoinResult:
+        self._apply_tuning(m, w)
         a = _f64(x)
         r = _Result()
         rc = load().dtwj_ctx_join(self._h, _dptr(a), a.size, m, w, flags, ctypes.byref(r))
@@ -347,6 +366,13 @@ class Context:
         rc = load().dtwj_ctx_set_band(self._h, w, C, G)
         if rc != OK:
             raise DtwjError(rc, "dtwj_ctx_set_band")
+
+    def set_tuning(self, dtw_warps: int = 0, chunk_tiles: int = 0):
+        """CTA size of the DTW kernel in warps (1, 2, 4, 8) and tiles per chunk
+        of the diagonal sweep (16..4096); 0 restores a default."""
+        rc = load().dtwj_ctx_set_tuning(self._h, dtw_warps, chunk_tiles)
+        if rc != OK:
+            raise DtwjError(rc, "dtwj_ctx_set_tuning")
 
     def set_model(self, net):
         """Network used by joins with F_LEARNED on this context (None clears)."""
@@ -379,6 +405,7 @@ class Context:
 
     def join_device(self, dev_ptr: int, n: int, m: int, w: int, flags: int = 0) -> JoinResult:
         """Join a series already in device memory (dev_ptr: n float64)."""
+        self._apply_tuning(m, w)
         r = _Result()
         rc = load().dtwj_ctx_join_device(self._h, ctypes.c_void_p(dev_ptr), n, m, w, flags,
                                          ctypes.byref(r))

@@ -222,6 +222,7 @@ __device__ __forceinline__ void kim_bound(const Seq& q, const Seq& t, int m, V* 
 struct BandShape {
   int C;  // cells (diagonals) per lane
   int G;  // lanes per pair
+  int warps = 0;  // CTA size of the join's DTW kernel in warps (0: the default, 4)
 };
 // The join's layout: one pair per warp (G = 32) with the fewest cells per
 // lane C in [2, 16] covering 2w+1 diagonals.  Returns false if w > 255.

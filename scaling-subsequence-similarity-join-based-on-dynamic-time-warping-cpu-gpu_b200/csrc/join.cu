@@ -81,6 +81,8 @@ struct dtwj_ctx {
   std::vector<Tile> tiles_run;             // the tiles in the order of the current call
   dtwj_mlp* model = nullptr;               // scores tiles for DTWJ_F_LEARNED (not owned)
   std::vector<std::pair<int, BandShape>> band_override;  // band w -> DTW layout (autotuner)
+  int dtw_warps = 0;    // CTA size of the join's DTW kernel in warps (0: default)
+  int chunk_tiles = 0;  // tiles per chunk of the sweep (0: default)
   int shard_rank = 0, shard_world = 1;  // this context sweeps tiles t with t % world == rank
   dtwj_exchange_fn exchange = nullptr;  // best-so-far exchange between sweep phases
   void* exchange_user = nullptr;
@@ -362,6 +364,7 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   if (!choose_band(w, &band)) return DTWJ_ERR_BAND;
   for (const auto& bo : ctx->band_override)
     if (bo.first == w) band = bo.second;
+  band.warps = ctx->dtw_warps;
   const bool learned = (flags & DTWJ_F_LEARNED) && !tq;
   if (learned && !ctx->model) return DTWJ_ERR_NOMODEL;
   if (learned && mlp_device(ctx->model) != ctx->device) return DTWJ_ERR_ARG;
@@ -523,7 +526,7 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   // ---- diagonal sweep in chunks of LB tiles ----
   const bool enumerate_all = flags & DTWJ_F_NO_DIAG;
   const double tile_pairs = (double)kLbLags * kLbRows;
-  int chunk = kLbChunkTiles;
+  int chunk = ctx->chunk_tiles > 0 ? ctx->chunk_tiles : kLbChunkTiles;
   if (enumerate_all) chunk = (int)((double)qcap / tile_pairs) > 0 ? (int)((double)qcap / tile_pairs) : 1;
   unsigned int* bits;
   ENSURE(B_BITS, (size_t)(chunk < nlb ? chunk : (nlb > 0 ? nlb : 1)) * kLbLags * kLbWords * 4, bits);
@@ -641,7 +644,7 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
         const unsigned char* b = static_cast<const unsigned char*>(p);
         key.insert(key.end(), b, b + bytes);
       };
-      const int band_cg[2] = {band.C, band.G};
+      const int band_cg[3] = {band.C, band.G, band.warps};
       const int64_t misc[11] = {nlb, chunk, enumerate_all, masked, cascade, ctx->num_sms, ph.on,
                                 (int64_t)ph.used, (int64_t)(uintptr_t)lbtiles,
                                 (int64_t)(uintptr_t)bits, (int64_t)(uintptr_t)notes};
@@ -909,6 +912,16 @@ int dtwj_ctx_set_band(dtwj_ctx* ctx, int32_t w, int32_t C, int32_t G) {
   if (C == 0 && G == 0) return DTWJ_OK;
   if (!band_shape_ok(w, C, G)) return DTWJ_ERR_BAND;
   v.push_back({w, BandShape{C, G}});
+  return DTWJ_OK;
+}
+
+int dtwj_ctx_set_tuning(dtwj_ctx* ctx, int32_t dtw_warps, int32_t chunk_tiles) {
+  if (!ctx) return DTWJ_ERR_ARG;
+  if (dtw_warps != 0 && dtw_warps != 1 && dtw_warps != 2 && dtw_warps != 4 && dtw_warps != 8)
+    return DTWJ_ERR_ARG;
+  if (chunk_tiles != 0 && (chunk_tiles < 16 || chunk_tiles > 4096)) return DTWJ_ERR_ARG;
+  ctx->dtw_warps = dtw_warps;
+  ctx->chunk_tiles = chunk_tiles;
   return DTWJ_OK;
 }
 

@@ -236,7 +236,7 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
 // The pair consumer: every group takes pairs from the queue until it is
 // drained.  flags bit 0: run the bounds (otherwise DTW only, for seeds).
 template <int C, int G>
-__global__ void __launch_bounds__(128) k_pairs(DevSeries S, DevSearch Q, const int2* pairs,
+__global__ void __launch_bounds__(256) k_pairs(DevSeries S, DevSearch Q, const int2* pairs,
                                                 const unsigned int* npairs, int flags,
                                                 int group_floats) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -501,12 +501,13 @@ __global__ void k_best_f32(const Candidate* cands, const unsigned int* count_ptr
 
 template <int C, int G>
 void run_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
-               const unsigned int* npairs, int flags, int num_sms, cudaStream_t st) {
+               const unsigned int* npairs, int flags, int num_sms, cudaStream_t st,
+               int warps) {
   const bool bounds = flags & 1;
   const GroupLayout lay = group_layout(S.m, S.w, C, G, bounds);
-  const int groups = 128 / G;
-  size_t bytes = (size_t)groups * lay.total * sizeof(float);
-  int threads = 128;
+  int threads = warps > 0 ? 32 * warps : 128;
+  if (threads < G) threads = G;
+  size_t bytes = (size_t)(threads / G) * lay.total * sizeof(float);
   // keep at least two blocks per SM when the series is long
   while (bytes > 100 * 1024 && threads > G && threads > 32) {
     threads /= 2;
@@ -630,7 +631,10 @@ void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
                   cudaStream_t st) {
   const int flags = bounds ? 1 : 0;
 #define X(c, g) \
-  if (band.C == c && band.G == g) { run_pairs<c, g>(S, Q, pairs, npairs, flags, num_sms, st); return; }
+  if (band.C == c && band.G == g) {                                               \
+    run_pairs<c, g>(S, Q, pairs, npairs, flags, num_sms, st, band.warps);          \
+    return;                                                                        \
+  }
   DTWJ_BAND_CASES(X)
 #undef X
 }

@@ -47,3 +47,24 @@ def test_tune_picks_the_fastest_and_caches(tmp_path):
     calls.clear()
     assert at.tune(256, 13, path, timer=timer) == saved["m=256,w=13"]
     assert not calls
+
+
+def test_tune_join_searches_each_knob_and_caches(tmp_path):
+    at = _autotune()
+    path = str(tmp_path / "tune.json")
+    calls = []
+
+    def measure(C, G, warps, chunk):
+        calls.append((C, G, warps, chunk))
+        # fastest: the layout with 64 cells, 8 warps, chunks of 256 tiles
+        return abs(C * G - 64) + (0 if warps == 8 else 1) + (0 if chunk == 256 else 1)
+
+    shapes = lambda w: [(2, 32), (4, 16), (7, 4)]
+    e = at.tune_join(None, 256, 13, path, measure=measure, shapes=shapes)
+    assert (e["C"], e["G"], e["dtw_warps"], e["chunk_tiles"]) == (2, 32, 8, 256)
+    assert len(calls) == 3 + 3 + 3 and len(e["tried"]) == 9
+    saved = json.load(open(path))
+    assert saved[at.join_key(256, 13)]["dtw_warps"] == 8
+    calls.clear()
+    assert at.tune_join(None, 256, 13, path, measure=measure, shapes=shapes) == saved[at.join_key(256, 13)]
+    assert not calls

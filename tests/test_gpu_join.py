@@ -374,3 +374,28 @@ def test_queue_overflow_sweeps_only_the_chunks_again(gpu_dtwj, synth):
         assert r.pairs == (s - m) * (s - m + 1) // 2
         total = r.pruned_fast + r.pruned_paa + r.pruned_kim + r.pruned_keogh + r.dtw_calls
         assert 0 <= total - r.pairs <= 700, (total, r.pairs)
+
+
+def test_tuned_join_equals_the_default(gpu_dtwj, synth, tmp_path):
+    # whole-join tuning (band layout, DTW CTA size, sweep chunk) on a sample,
+    # applied by a context created with the cache: same result as the default
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "dtwj.autotune", os.path.join(PKG_DIR, "autotune.py"))
+    at = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(at)
+    x = synth.ecg_like(12000, 5)
+    m, w = 128, 7
+    path = str(tmp_path / "join_tune.json")
+    e = at.tune_join(x[:6000].copy(), m, w, path, warps=(1, 8), chunks=(16, 2048))
+    assert e["dtw_warps"] in (1, 8) and e["chunk_tiles"] in (16, 2048)
+    assert all(t[4] > 0 for t in e["tried"])
+    with gpu_dtwj.Context() as ctx:
+        plain = ctx.join(x, m, w)
+    with gpu_dtwj.Context(tune_cache=path) as ctx:
+        tuned = ctx.join(x, m, w)
+        assert (tuned.i, tuned.j, tuned.dist) == (plain.i, plain.j, plain.dist)
+        assert tuned.pairs == plain.pairs
+        for bad in ((3, 0), (0, 8), (0, 5000)):
+            with pytest.raises(gpu_dtwj.DtwjError):
+                ctx.set_tuning(*bad)
