@@ -147,6 +147,10 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const bf16
                                           ~static_cast<uintptr_t>(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTcRows;
+  // split K (weight gradients: K = the batch rows): CTA y takes [k_beg, k_end)
+  const int k_per = (K + (int)gridDim.y * kTcK - 1) / ((int)gridDim.y * kTcK) * kTcK;
+  const int k_beg = (int)blockIdx.y * k_per;
+  const int k_end = k_beg + k_per < K ? k_beg + k_per : K;
   const uint32_t a_base = smem_u32(sh.a), b_base = smem_u32(sh.b), mbar = smem_u32(&sh.mbar);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -165,14 +169,14 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const bf16
   const bf16 z = __float2bfloat16(0.0f);
   uint32_t phase = 0;
   bool ok = true;
-  for (int k0 = 0; k0 < K && ok; k0 += kTcK) {
+  for (int k0 = k_beg; k0 < k_end && ok; k0 += kTcK) {
     tc_stage(reinterpret_cast<unsigned char*>(sh.a), kTcRows, tid, [&](int r, int k) {
       const int m = m0 + r, kk = k0 + k;
-      return (m < M && kk < K) ? A[m * sam + kk * sak] : z;
+      return (m < M && kk < k_end) ? A[m * sam + kk * sak] : z;
     });
     tc_stage(reinterpret_cast<unsigned char*>(sh.b), N, tid, [&](int n, int k) {
       const int kk = k0 + k;
-      return kk < K ? B[kk * sbk + n * sbn] : z;
+      return kk < k_end ? B[kk * sbk + n * sbn] : z;
     });
     // the tiles written by ordinary stores become visible to the tensor cores
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -182,7 +186,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const bf16
 #pragma unroll
       for (int s = 0; s < kTcK / 16; ++s) {
         const uint64_t ad = tc_desc(a_base + s * 2 * kTcLbo), bd = tc_desc(b_base + s * 2 * kTcLbo);
-        const uint32_t acc = (k0 > 0 || s > 0) ? 1u : 0u;
+        const uint32_t acc = (k0 > k_beg || s > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
@@ -197,7 +201,8 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const bf16
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const int row = m0 + warp * 32 + lane;
-  for (int c0 = 0; c0 < N; c0 += 32) {
+  // a split-K CTA whose range is empty has no accumulator to add
+  for (int c0 = 0; c0 < N && k_beg < k_end; c0 += 32) {
     uint32_t v[32];
     if (ok) tc_load32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
     if (row < M) {
@@ -205,7 +210,8 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const bf16
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         const float x = ok ? __uint_as_float(v[j]) : __int_as_float(0x7fc00000);
-        c[j] = accumulate ? c[j] + x : x;
+        if (gridDim.y > 1) atomicAdd(c + j, x);  // split K: C was cleared or holds the sum
+        else c[j] = accumulate ? c[j] + x : x;
       }
     }
   }
@@ -365,7 +371,13 @@ void gemm(bool precise, int M, int N, int K, const void* A, int64_t sam, int64_t
     k_gemm_f32<<<grid_for((int64_t)M * N), kThreads, 0, st>>>(
         M, N, K, (const float*)A, sam, sak, (const float*)B, sbk, sbn, C, ldc, acc);
   } else {
-    k_gemm_tc<<<(unsigned)((M + kTcRows - 1) / kTcRows), 128, kTcSmemBytes, st>>>(
+    // long K on few rows (the weight gradients): split K over CTAs that add
+    // their products into C, cleared first unless accumulating
+    const int mblocks = (M + kTcRows - 1) / kTcRows;
+    int ksplit = 1;
+    if (mblocks == 1 && K >= 1024) ksplit = K / 512 < 64 ? K / 512 : 64;
+    if (ksplit > 1 && !acc) cudaMemsetAsync(C, 0, (size_t)M * ldc * sizeof(float), st);
+    k_gemm_tc<<<dim3((unsigned)mblocks, (unsigned)ksplit), 128, kTcSmemBytes, st>>>(
         M, N, K, (const bf16*)A, sam, sak, (const bf16*)B, sbk, sbn, C, ldc, acc, status);
   }
 }
