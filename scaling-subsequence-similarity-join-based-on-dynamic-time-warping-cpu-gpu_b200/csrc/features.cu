@@ -92,7 +92,8 @@ __global__ void k_tile_features(DevSeries S, const Tile* tiles, int ntiles,
   for (int k = 0; k < 8; ++k) {
     const int a = k * T.rows / 8, b = (k + 1) * T.rows / 8;
     double mn = INF, cnt = 0.0;
-    for (int r = a + lane; r < b; r += 32) {
+    // only the keyed rows (every row, or the seed profile's grid rows)
+    for (int r = (a + grid - 1) / grid * grid + lane * grid; r < b; r += 32 * grid) {
       const int64_t i = T.i0 + r;
       const unsigned long long key = keys[i];
       mn = fmin(mn, mp_value(key, inv_norm));

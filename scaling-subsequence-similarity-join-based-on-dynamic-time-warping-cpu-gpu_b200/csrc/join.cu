@@ -15,6 +15,8 @@
 #include "../../include/dtwj.h"
 #include "dtwj_dev.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -54,6 +56,26 @@ struct ChunkNote {
   unsigned int overflow;
   unsigned int pad;
 };
+
+// Sort keys of the learned order: ascending score, NaN last; the radix sort
+// is stable, so ties keep the plain order.
+__global__ void k_order_keys(const float* score, int n, unsigned int* key, int* idx) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const float f = score[t];
+  const unsigned int u = __float_as_uint(f);
+  key[t] = f != f ? 0xffffffffu : ((u & 0x80000000u) ? ~u : (u | 0x80000000u));
+  idx[t] = t;
+}
+
+// Tiles in the sorted order, each with its position.
+__global__ void k_gather_tiles(const Tile* plain, const int* idx, int n, Tile* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  Tile x = plain[idx[t]];
+  x.order = t;
+  out[t] = x;
+}
 
 // Runs after a chunk's last stage on the join's stream: notes the chunk and
 // clears the overflow bit for the next one.
@@ -106,7 +128,7 @@ enum BufId {
   B_MP, B_MPI, B_CB, B_AF, B_ULF, B_BITS, B_LBTILES, B_KQ, B_SBEG, B_SID, B_SEEDBSF,
   B_BEST_IJ, B_BEST_F32, B_QSER, B_TILEBEST, B_FEAT, B_SCORE, B_PA, B_CMAX, B_RW,
   B_MPX_WANT, B_MPX_WREV, B_MPX_MIN, B_MPX_IDX, B_MPX_CAND, B_MPX_CNT, B_NOTES, B_NOTES2,
-  B_COUNT_
+  B_SORT, B_SORT_TEMP, B_LBTILES2, B_COUNT_
 };
 
 int ensure(dtwj_ctx* c, int id, size_t bytes, void** out) {
@@ -478,23 +500,28 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
       ENSURE(B_SCORE, (size_t)nlb * 4, score);
       rc = mlp_predict_device(ctx->model, feat, nlb, score, st);
       if (rc) return rc;
-      std::vector<float> sc((size_t)nlb);
-      CUDA_OK(cudaMemcpy(sc.data(), score, (size_t)nlb * 4, cudaMemcpyDeviceToHost));
-      std::vector<int> ord((size_t)nlb);
-      for (int t = 0; t < nlb; ++t) ord[t] = t;
-      // ascending predicted minimum; ties (and NaN scores, last) keep the plain order
-      std::stable_sort(ord.begin(), ord.end(), [&sc](int a, int b) {
-        const bool na = !(sc[a] == sc[a]), nb = !(sc[b] == sc[b]);
-        if (na != nb) return nb;
-        return !na && sc[a] < sc[b];
-      });
-      const std::vector<Tile> plain = th;
-      for (int t = 0; t < nlb; ++t) {
-        th[t] = plain[ord[t]];
-        th[t].order = t;
-      }
-      CUDA_OK(cudaMemcpyAsync(lbtiles, th.data(), (size_t)nlb * sizeof(Tile),
-                              cudaMemcpyHostToDevice, st));
+      // ascending predicted minimum; ties (and NaN scores, last) keep the
+      // plain order: a stable radix sort of (score key, tile) on the device,
+      // then the tiles gathered in that order
+      unsigned int* sk;
+      ENSURE(B_SORT, (size_t)nlb * 16, sk);
+      unsigned int* sk_out = sk + nlb;
+      int* si = reinterpret_cast<int*>(sk + 2 * (size_t)nlb);
+      int* si_out = si + nlb;
+      const unsigned int nb = (unsigned int)((nlb + 255) / 256);
+      k_order_keys<<<nb, 256, 0, st>>>(score, nlb, sk, si);
+      size_t temp_bytes = 0;
+      CUDA_OK(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, sk, sk_out, si, si_out, nlb,
+                                              0, 32, st));
+      void* temp;
+      ENSURE(B_SORT_TEMP, temp_bytes > 0 ? temp_bytes : 16, temp);
+      CUDA_OK(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, sk, sk_out, si, si_out, nlb, 0,
+                                              32, st));
+      Tile* sorted;
+      ENSURE(B_LBTILES2, (size_t)nlb * sizeof(Tile), sorted);
+      k_gather_tiles<<<nb, 256, 0, st>>>(lbtiles, si_out, nlb, sorted);
+      CUDA_OK(cudaMemcpyAsync(lbtiles, sorted, (size_t)nlb * sizeof(Tile),
+                              cudaMemcpyDeviceToDevice, st));
     }
   }
   if (tq && !tile_mode) {
