@@ -15,11 +15,13 @@
 // G lanes computes one pair; lane g owns the C consecutive diagonals
 // d = -w + gC .. -w + gC + C - 1 (cell (r, r + d)).  Lane g handles row
 // r = tau - g at step tau: cell (r, d) needs (r, d-1) from the left lane's
-// previous step (shfl_up of its last cell) and (r-1, d+1) from the right
-// lane's first cell of this step (shfl_down right after it is computed), so
+// previous step (a shuffle of its last cell) and (r-1, d+1) from the right
+// lane's first cell of this step (a shuffle right after it is computed), so
 // every lane computes a full row of its C cells per step with two shuffles.
-// q and t are z-normalised in shared memory with finite sentinels outside
-// [0, m) so out-of-range cells are effectively infinite without branches.
+// The join runs one pair per warp (G = 32); pair lists pack several.  q and t
+// are z-normalised in shared memory with finite sentinels outside [0, m) so
+// out-of-range cells are effectively infinite without branches; a lane keeps
+// the q and t values of C consecutive steps in registers.
 #include "dtwj_dev.cuh"
 
 #include <cfloat>
@@ -102,7 +104,7 @@ __host__ __device__ inline GroupLayout group_layout(int m, int w, int C, int G, 
 // elsewhere), exactly what row 0 needs.
 template <typename T, int C, int G, typename TW>
 __device__ __forceinline__ void band_step(T qr, const TW& tw, bool live, int g, unsigned int gm,
-                                          T INF, const T (&pen)[C], T (&A)[C]) {
+                                          const T (&pen)[C], T (&A)[C]) {
   // Lane 0's left neighbour and lane G-1's right neighbour wrap around the
   // group, so no lane needs a select: C G is even and 2w + 1 odd, so C G >
   // 2w + 1 and lane G-1's last cell lies past the band; its +inf penalty
@@ -163,7 +165,7 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
   int tau = 0;
   for (; tau < warm; ++tau) {
     const T* tp = tg + tau;
-    band_step<T, C, G>(qg[tau], [tp](int c) { return tp[c]; }, tau - g >= 0, g, gm, INF, pen, A);
+    band_step<T, C, G>(qg[tau], [tp](int c) { return tp[c]; }, tau - g >= 0, g, gm, pen, A);
   }
   // blocks of C steps with q and t in registers
   constexpr int kAbEvery = (16 + C - 1) / C;  // blocks between abandon checks
@@ -186,7 +188,7 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
     qb += C;
 #pragma unroll
     for (int k = 0; k < C; ++k)
-      band_step<T, C, G>(Qv[k], [&W, k](int c) { return W[k + c]; }, true, g, gm, INF, pen, A);
+      band_step<T, C, G>(Qv[k], [&W, k](int c) { return W[k + c]; }, true, g, gm, pen, A);
 #pragma unroll
     for (int x = 0; x < C - 1; ++x) W[x] = W[x + C];
     tau += C;
@@ -222,7 +224,7 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
   // the last steps (fewer than C)
   for (; tau <= tau_end; ++tau) {
     const T* tp = tg + tau;
-    band_step<T, C, G>(qg[tau], [tp](int c) { return tp[c]; }, true, g, gm, INF, pen, A);
+    band_step<T, C, G>(qg[tau], [tp](int c) { return tp[c]; }, true, g, gm, pen, A);
   }
   T result = INF;
 #pragma unroll
