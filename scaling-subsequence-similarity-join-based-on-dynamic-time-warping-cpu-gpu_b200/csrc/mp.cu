@@ -222,8 +222,9 @@ static_assert(kSeedGrid == kLbPerThread, "grid rows are the first of each unroll
 static_assert(kLbRows % kSeedGrid == 0 && kStage % kSeedGrid == 0, "tiles and stages on the grid");
 
 struct MpSeedShared {
-  float p1[kCols], p2[kCols], is[kCols], c2[kCols];
-  float r1[kStage], r2[kStage], ci[kStage];
+  float2 p[kCols];   // (dfa, dga) of column j - 1: one 8-byte read per row and thread
+  float is[kCols], c2[kCols];
+  float4 r[kStage];  // (dfa, dga of row i - 1, -2 isg of row i, 0): one broadcast read per row
   unsigned long long rowbest[kStage / kSeedGrid];
 };
 
@@ -269,25 +270,24 @@ __global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Ti
     for (int x = t; x < kCols; x += kLbThreads) {
       const int64_t j = c0 + x;
       const bool in = j >= 0 && j < s, up = j >= 1 && j < s;
-      sh.p1[x] = up ? (float)S.dfa[j - 1] : 0.0f;
-      sh.p2[x] = up ? (float)S.dga[j - 1] : 0.0f;
+      sh.p[x] = make_float2(up ? (float)S.dfa[j - 1] : 0.0f, up ? (float)S.dga[j - 1] : 0.0f);
       sh.is[x] = in ? (float)S.isg[j] : 0.0f;
       sh.c2[x] = (in && !S.flat[j]) ? two_m : 1e30f;
     }
     for (int x = t; x < kStage; x += kLbThreads) {
       const int64_t i = r0 + x;
       const bool in = i >= 0 && i < s, up = i >= 1 && i < s;
-      sh.r1[x] = up ? (float)S.dfa[i - 1] : 0.0f;
-      sh.r2[x] = up ? (float)S.dga[i - 1] : 0.0f;
-      sh.ci[x] = (in && !S.flat[i]) ? (float)(-2.0 * S.isg[i]) : 0.0f;
+      sh.r[x] = make_float4(up ? (float)S.dfa[i - 1] : 0.0f, up ? (float)S.dga[i - 1] : 0.0f,
+                            (in && !S.flat[i]) ? (float)(-2.0 * S.isg[i]) : 0.0f, 0.0f);
     }
     __syncthreads();
     const int cb = t * kLbPerThread;
     float Cb[kLbPerThread], D[kLbPerThread];
 #pragma unroll
     for (int l = 0; l < kLbPerThread; ++l) {
-      w1[l] = sh.p1[cb + l];
-      w2[l] = sh.p2[cb + l];
+      const float2 pc = sh.p[cb + l];
+      w1[l] = pc.x;
+      w2[l] = pc.y;
       Cb[l] = (float)C[l];
       D[l] = 0.0f;
     }
@@ -296,7 +296,8 @@ __global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Ti
       for (int u = 0; u < kLbPerThread; ++u) {
         const int r = qq * kLbPerThread + u;
         const bool first = (st == 0 && r == 0);
-        const float q1 = sh.r1[r], q2 = sh.r2[r];
+        const float4 rq = sh.r[r];
+        const float q1 = rq.x, q2 = rq.y;
         if (!first) {
 #pragma unroll
           for (int l = 0; l < kLbPerThread; ++l) {
@@ -307,7 +308,7 @@ __global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Ti
         }
         // a grid row (u == 0: lag l's column sits in ring slot l and at
         // stage column cb + r + l)
-        const float qc = sh.ci[r];
+        const float qc = rq.z;
         if (u == 0 && st + r < T.rows && qc != 0.0f) {
           unsigned int best = UINT_MAX;
 #pragma unroll
@@ -331,8 +332,9 @@ __global__ void __launch_bounds__(kLbThreads, 6) k_mp_seed(DevSeries S, const Ti
           }
         }
         const int nx = cb + r + kLbPerThread;
-        w1[u] = sh.p1[nx];
-        w2[u] = sh.p2[nx];
+        const float2 pn = sh.p[nx];
+        w1[u] = pn.x;
+        w2[u] = pn.y;
       }
     }
 #pragma unroll
