@@ -106,6 +106,9 @@ constexpr int kRunMax = 256;
 // 2^kBlkShift samples (value minus the block mean) so that the float rounding
 // error stays far below the pruning slack.
 constexpr int kBlkShift = 10;
+// Blocks of each copy of DevSeries::pq2 (copy 1's block b starts 1024
+// samples before copy 0's).
+__host__ __device__ inline int64_t kCopyBlocks(int64_t n) { return (n >> 11) + 2; }
 
 // Counters, all uint64 on the device.
 enum Counter {
@@ -163,9 +166,18 @@ struct DevSeries {
   float2* ulf;      // n, (U - cb[block], L - cb[block])
   int paa_b;        // block length of the block-mean bound (8, 16 or 32)
   float4* pq;       // n, means over [p, p + paa_b) of (a, U, L) - cb[block of p], 0
+                    //    (windows longer than 1024 samples; else nullptr)
   float* cmax;      // (n >> kBlkShift) + 2, largest |centered FP32 value| per block
   float* rw;        // s, FP32 error scale of window i: isg_i x the largest
                     //    centered magnitude or block offset its FP32 bounds read
+  // Windows of at most 1024 samples: the same block means in two copies
+  // centered per 2048-sample block, copy 0 on [2048 b, 2048 b + 2048) and
+  // copy 1 on [2048 b - 1024, 2048 b + 1024), so every window lies inside one
+  // block of one copy and has a single block offset (else all nullptr).
+  float4* pq2;      // 2n, copy c at [c n, c n + n)
+  float* cmax2;     // 2 kCopyBlocks(n), largest |value| of each copy block
+  float4* wrec;     // s, window record: block offset (FP64 in .x/.y), isg as
+                    //    FP32 (.z) and the error scale for pq2 (.w)
   int* status;      // device status word (0 ok, else error bits)
 };
 
@@ -314,9 +326,10 @@ void launch_paa(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int t
                 int tile_end, const unsigned int* bits, int num_sms, cudaStream_t st);
 // Block length of the block-mean bound for windows of length m.
 int paa_block(int m);
-// Sliding block means (pq), per-block magnitudes (cmax) and per-window
-// error scales (rw); after launch_center.
-void launch_paa_prep(const DevSeries& S, cudaStream_t st);
+// Sliding block means (pq, or pq2 and wrec for windows of at most 1024
+// samples), per-block magnitudes (cmax) and per-window error scales (rw);
+// after launch_center.  Returns the number of kernels it launched.
+int launch_paa_prep(const DevSeries& S, cudaStream_t st);
 // LB_Keogh over the candidates the run filter queued in Q.kq; survivors go to
 // Q.queue.
 void launch_keogh(const DevSeries& S, const DevSearch& Q, int num_sms, cudaStream_t st);

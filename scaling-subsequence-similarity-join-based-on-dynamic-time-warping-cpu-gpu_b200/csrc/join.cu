@@ -128,7 +128,7 @@ enum BufId {
   B_MP, B_MPI, B_CB, B_AF, B_ULF, B_BITS, B_LBTILES, B_KQ, B_SBEG, B_SID, B_SEEDBSF,
   B_BEST_IJ, B_BEST_F32, B_QSER, B_TILEBEST, B_FEAT, B_SCORE, B_PA, B_CMAX, B_RW,
   B_MPX_WANT, B_MPX_WREV, B_MPX_MIN, B_MPX_IDX, B_MPX_CAND, B_MPX_CNT, B_NOTES, B_NOTES2,
-  B_SORT, B_SORT_TEMP, B_LBTILES2, B_COUNT_
+  B_SORT, B_SORT_TEMP, B_LBTILES2, B_CMAX2, B_WREC, B_COUNT_
 };
 
 int ensure(dtwj_ctx* c, int id, size_t bytes, void** out) {
@@ -303,7 +303,13 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   ENSURE(B_CB, ((n >> kBlkShift) + 4) * 8, S.cb);
   ENSURE(B_AF, n * 4, S.af);
   ENSURE(B_ULF, n * 8, S.ulf);
-  ENSURE(B_PA, n * 16, S.pq);
+  if (m <= (1 << kBlkShift)) {
+    ENSURE(B_PA, (size_t)n * 32, S.pq2);
+    ENSURE(B_CMAX2, (size_t)kCopyBlocks(n) * 8, S.cmax2);
+    ENSURE(B_WREC, (size_t)s * 16, S.wrec);
+  } else {
+    ENSURE(B_PA, (size_t)n * 16, S.pq);
+  }
   ENSURE(B_CMAX, ((n >> kBlkShift) + 4) * 4, S.cmax);
   ENSURE(B_RW, s * 4, S.rw);
   S.paa_b = paa_block(m);
@@ -355,8 +361,8 @@ int prepare(dtwj_ctx* ctx, const double* x_dev, int64_t n, int m, int w, bool ma
   }
   launch_rowterms(S, masked, st);
   launch_center(S, st);
-  launch_paa_prep(S, st);
-  if (ph) ph->end(DTWJ_PHASE_PREP, masked ? 14 : 9);
+  const int paa_launches = launch_paa_prep(S, st);
+  if (ph) ph->end(DTWJ_PHASE_PREP, (masked ? 11 : 6) + paa_launches);
   CUDA_OK(cudaGetLastError());
   *out = S;
   return DTWJ_OK;

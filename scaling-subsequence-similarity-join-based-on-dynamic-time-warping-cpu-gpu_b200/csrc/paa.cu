@@ -15,9 +15,11 @@
 // diagonal bound and endpoint bound prune about 86 %.
 //
 // Work items are (tile, 32-row word, group of 32 lags) of the diagonal
-// sweep's survivor bits, stored [tile][word][lag].  A warp loads the 32 words
-// of its lag group in one coalesced read; for every lag L with survivors,
-// lane p takes row i = i0 + p of the word (survivors cluster: a nonzero word
+// sweep's survivor bits, stored [tile][word][lag].  Windows of at most 1024
+// samples go to k_paa_lags (lanes on lags, described there).  For longer
+// ones (k_paa), a warp loads the 32 words of its lag group in one coalesced
+// read; for every lag L with survivors, lane p takes row i = i0 + p of the
+// word (survivors cluster: a nonzero word
 // holds about 28 of 32 rows).  The blocks are aligned to absolute sample
 // positions: block [x, x + B) of window i, x a multiple of B, meets block
 // [x + L, x + L + B) of window j, so every lane of the batch reads the same
@@ -33,10 +35,14 @@
 // endpoint bound (LB_Kim, CPU_version1/lb_kim.cpp:10-73) then runs in FP64 on
 // the survivors, which go to the LB_Keogh queue.
 //
-// Precision: the sliding means are FP32, centered per 1024-sample block like
-// the LB_Keogh copies, and normalised per window by an FP64 block offset.  A
-// pair is pruned only when the FP32 error bound of its windows (rw) fits in
-// the slack the threshold keeps above the best-so-far (fp32_bound_ok).
+// Precision: the sliding means are FP32, centered per block, and normalised
+// per window by an FP64 block offset.  For windows longer than 1024 samples
+// the blocks are the 1024-sample blocks of the LB_Keogh copies; for shorter
+// ones, 2048-sample blocks in two copies shifted by 1024 samples, so that a
+// window lies in one block (one offset per window).  A pair is pruned only
+// when the FP32 error bound of its windows (rw, or the window record's scale)
+// fits in the slack the threshold keeps above the best-so-far
+// (fp32_bound_ok).
 #include "../../include/dtwj.h"
 #include "dtwj_dev.cuh"
 
@@ -51,15 +57,35 @@ __device__ __forceinline__ float max3f(float a, float b, float c) {
   return d;
 }
 
-// Sliding block means, centered on the 1024-sample block of their first
-// sample: pq[p] = (means over [p, p + B) of a, U, L) - cb[p >> kBlkShift].
-// Entries whose block runs past the series are zero (never read: a window's
-// blocks end inside it).
+// Centers of the two copies of the block means for windows of at most 1024
+// samples: block b of copy 0 is [2048 b, 2048 b + 2048), block b of copy 1 is
+// [2048 b - 1024, 2048 b + 1024); each is centered on the mean of the two
+// 1024-sample blocks it spans (cb, padded past the end).
+__device__ __forceinline__ int64_t copy_block(int copy, int64_t p) { return (p + copy * 1024) >> 11; }
+__device__ __forceinline__ double copy_center(const DevSeries& S, int copy, int64_t b) {
+  const int64_t k = 2 * b - copy;
+  return k < 0 ? S.cb[0] : 0.5 * (S.cb[k] + S.cb[k + 1]);
+}
+// The copy whose blocks hold window [i, i + m), m <= 1024: copy 0 when the
+// window ends inside its 2048-sample block, else copy 1 (then i mod 2048 >
+// 1024 and the window lies in [2048 b + 1024, 2048 b + 3072)).
+__device__ __forceinline__ int win_copy(int64_t i, int m) { return (int)(i & 2047) + m > 2048 ? 1 : 0; }
+
+// Sliding block means over [p, p + B) of a, U and L, centered: on the
+// 1024-sample block of p (pq, windows longer than 1024 samples), or on the
+// block of p in each of the two copies (pq2).  Entries whose block runs past
+// the series are zero (never read: a window's blocks end inside it).
 __global__ void k_slide_means(DevSeries S, int B) {
   const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= S.n) return;
   if (p + B > S.n) {
-    S.pq[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (S.pq2) {
+      S.pq2[p] = z;
+      S.pq2[S.n + p] = z;
+    } else {
+      S.pq[p] = z;
+    }
     return;
   }
   double sa = 0.0, su = 0.0, sl = 0.0;
@@ -68,12 +94,32 @@ __global__ void k_slide_means(DevSeries S, int B) {
     su += S.U[p + k];
     sl += S.L[p + k];
   }
-  const double c = S.cb[p >> kBlkShift], ib = 1.0 / (double)B;
-  S.pq[p] = make_float4((float)(sa * ib - c), (float)(su * ib - c), (float)(sl * ib - c), 0.0f);
+  const double ib = 1.0 / (double)B;
+  const double ma = sa * ib, mu = su * ib, ml = sl * ib;
+  if (S.pq2) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const double x = copy_center(S, c, copy_block(c, p));
+      S.pq2[c * S.n + p] = make_float4((float)(ma - x), (float)(mu - x), (float)(ml - x), 0.0f);
+    }
+  } else {
+    const double x = S.cb[p >> kBlkShift];
+    S.pq[p] = make_float4((float)(ma - x), (float)(mu - x), (float)(ml - x), 0.0f);
+  }
+}
+
+__device__ __forceinline__ float block_max_reduce(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __shared__ float red[8];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  float t = 0.0f;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = fmaxf(t, red[w]);
+  return t;
 }
 
 // cmax[b] = the largest magnitude of any centered FP32 value of block b
-// (af, ulf, pq), read by LB_Keogh and the block-mean bound.
+// (af, ulf and, when built, pq), read by LB_Keogh and the block-mean bound.
 __global__ void k_block_max(DevSeries S, int nb) {
   const int b = blockIdx.x;
   if (b >= nb) return;
@@ -83,19 +129,33 @@ __global__ void k_block_max(DevSeries S, int nb) {
   float v = 0.0f;
   for (int64_t p = lo + threadIdx.x; p < hi; p += blockDim.x) {
     const float2 u = S.ulf[p];
-    const float4 q = S.pq[p];
     v = fmaxf(v, fmaxf(fabsf(S.af[p]), fmaxf(fabsf(u.x), fabsf(u.y))));
-    v = fmaxf(v, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
+    if (S.pq) {
+      const float4 q = S.pq[p];
+      v = fmaxf(v, fmaxf(fabsf(q.x), fmaxf(fabsf(q.y), fabsf(q.z))));
+    }
   }
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  __shared__ float red[8];
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float t = 0.0f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = fmaxf(t, red[w]);
-    S.cmax[b] = t;
+  const float t = block_max_reduce(v);
+  if (threadIdx.x == 0) S.cmax[b] = t;
+}
+
+// cmax2[c * kCopyBlocks + b] = the largest magnitude of pq2 over block b of
+// copy c (grid: 2 kCopyBlocks(n) blocks).
+__global__ void k_block_max2(DevSeries S) {
+  const int64_t nbc = kCopyBlocks(S.n);
+  const int c = (int)(blockIdx.x / nbc);
+  const int64_t b = blockIdx.x - c * nbc;
+  int64_t lo = b * 2048 - c * 1024, hi = lo + 2048;
+  if (lo < 0) lo = 0;
+  if (hi > S.n) hi = S.n;
+  const float4* q = S.pq2 + c * S.n;
+  float v = 0.0f;
+  for (int64_t p = lo + threadIdx.x; p < hi; p += blockDim.x) {
+    const float4 x = q[p];
+    v = fmaxf(v, fmaxf(fabsf(x.x), fmaxf(fabsf(x.y), fabsf(x.z))));
   }
+  const float t = block_max_reduce(v);
+  if (threadIdx.x == 0) S.cmax2[blockIdx.x] = t;
 }
 
 // rw[i] = isg_i * max over the blocks window i covers of (cmax[b] +
@@ -108,6 +168,22 @@ __global__ void k_window_scale(DevSeries S) {
   double r = 0.0;
   for (int64_t b = b0; b <= b1; ++b) r = fmax(r, (double)S.cmax[b] + fabs(S.cb[b] - mu));
   S.rw[i] = (float)(r * S.isg[i] * (1.0 + 1e-6));
+}
+
+// Window records for pq2: the block offset (x_c - mu_i) isg_i of the copy
+// block holding window i (center x_c), FP64; isg_i as FP32; and the error
+// scale isg_i (cmax2 + |x_c - mu_i|) of the values the block-mean bound forms
+// for it (the rw of pq2).
+__global__ void k_window_rec(DevSeries S) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= S.s) return;
+  const int c = win_copy(i, S.m);
+  const int64_t b = copy_block(c, i);
+  const double x = copy_center(S, c, b), mu = S.mu[i], is = S.isg[i];
+  const double off = (x - mu) * is;
+  const double r = ((double)S.cmax2[c * kCopyBlocks(S.n) + b] + fabs(x - mu)) * is * (1.0 + 1e-6);
+  S.wrec[i] = make_float4(__int_as_float(__double2loint(off)), __int_as_float(__double2hiint(off)),
+                          (float)is, (float)r);
 }
 
 // Scaled block offset of window x at 1024-sample block b, FP64.
@@ -304,10 +380,10 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 3) k_paa(DevSeries S, DevSearc
 // window (block k: [i + kB, i + kB + B)); its block means are the same for
 // every lane (broadcast loads) and the partner's [j + kB, j + kB + B), j =
 // i + L, sit at consecutive lags (coalesced loads), so no lane needs blocks
-// of its own at the window ends.  A window of at most 1024 samples meets at
-// most two 1024-sample blocks, so a pair's block offset takes one of three
-// values along the window (before either side changes block, after one, after
-// both), computed once per batch in FP64.  The blocks run in a stride-4 order
+// of its own at the window ends.  The means come from pq2, where every window
+// lies inside one block of one copy: a pair's block offset is one FP32 value,
+// the difference of its windows' FP64 offsets (wrec), and a block term is
+// two loads and ten FP32 operations.  The blocks run in a stride-4 order
 // (k = 0, 4, 8, ..., then 1, 5, 9, ...), which spreads the first terms over
 // the whole window: on the bench series a batch is settled after 7.6 blocks
 // on average against 9.2 in position order (CPU measurement over sampled lag
@@ -356,22 +432,14 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 3) k_paa_lags(DevSeries S, Dev
       // a lane without a pair computes the first live lane's pair (valid
       // addresses, result ignored), so the block loop needs no predicate
       const int j = i + (live ? L : L - lane + __ffs(lm) - 1);
-      const double mi = S.mu[i], si = S.isg[i];
-      const double mj = S.mu[j], sj = S.isg[j];
-      const float thr_lane = live && S.rw[i] <= r_ok && S.rw[j] <= r_ok ? thr : INF;
-      // block offsets: i's window starts in 1024-block bi and moves to bi + 1
-      // at block ki; j's likewise at kj
-      const int bi = i >> kBlkShift, bj = j >> kBlkShift;
-      const int ki = (((bi + 1) << kBlkShift) - i + B - 1) / B;
-      const int kj = (((bj + 1) << kBlkShift) - j + B - 1) / B;
-      const double oi0 = win_offset(S, bi, mi, si), oi1 = win_offset(S, bi + 1, mi, si);
-      const double oj0 = win_offset(S, bj, mj, sj), oj1 = win_offset(S, bj + 1, mj, sj);
-      const int k_lo = ki < kj ? ki : kj, k_hi = ki < kj ? kj : ki;
-      const float o_lo = (float)(oi0 - oj0), o_hi = (float)(oi1 - oj1);
-      const float o_mid = (float)(ki < kj ? oi1 - oj0 : oi0 - oj1);
-      const float fsi = (float)si, fsj = (float)sj;
-      const float4* pi = S.pq + i;  // broadcast: one read for the warp
-      const float4* pj = S.pq + j;  // consecutive lags: coalesced
+      const float4 wri = S.wrec[i];  // broadcast
+      const float4 wrj = S.wrec[j];  // consecutive lags: coalesced
+      const float thr_lane = live && wri.w <= r_ok && wrj.w <= r_ok ? thr : INF;
+      const float o = (float)(__hiloint2double(__float_as_int(wri.y), __float_as_int(wri.x)) -
+                              __hiloint2double(__float_as_int(wrj.y), __float_as_int(wrj.x)));
+      const float fsi = wri.z, fsj = wrj.z;
+      const float4* pi = S.pq2 + (win_copy(i, m) ? S.n : 0) + i;
+      const float4* pj = S.pq2 + (win_copy(j, m) ? S.n : 0) + j;
       float acc1 = 0.0f, acc2 = 0.0f;
       bool pruned = !live;
       // stride-4 order, a vote after every four blocks
@@ -383,27 +451,23 @@ __global__ void __launch_bounds__(kPaaWarps * 32, 3) k_paa_lags(DevSeries S, Dev
         const float4* qj = pj + r4 * B;
         for (; k + 12 < nb; k += 16, qi += 16 * B, qj += 16 * B) {
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int kk = k + 4 * u;
-            const float o = kk < k_lo ? o_lo : (kk < k_hi ? o_mid : o_hi);
-            block_terms(qi[4 * u * B], qj[4 * u * B], fsi, fsj, o, acc1, acc2);
-          }
+          for (int u = 0; u < 4; ++u) block_terms(qi[4 * u * B], qj[4 * u * B], fsi, fsj, o, acc1, acc2);
           pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
           if (__all_sync(0xffffffffu, pruned)) break;
         }
         if (k + 12 < nb) break;  // every lane pruned
-        for (; k < nb; k += 4, qi += 4 * B, qj += 4 * B) {
-          const float o = k < k_lo ? o_lo : (k < k_hi ? o_mid : o_hi);
-          block_terms(qi[0], qj[0], fsi, fsj, o, acc1, acc2);
+        if (k < nb) {
+          for (; k < nb; k += 4, qi += 4 * B, qj += 4 * B) block_terms(qi[0], qj[0], fsi, fsj, o, acc1, acc2);
+          pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
+          if (__all_sync(0xffffffffu, pruned)) break;
         }
-        pruned = pruned || (float)B * fmaxf(acc1, acc2) > thr_lane;
-        if (__all_sync(0xffffffffu, pruned)) break;
       }
       bool alive = live && !pruned;
       npaa += (live && pruned) ? 1u : 0u;
       float kim = 0.0f;
       if (alive) {
         // endpoint bound on the survivors (FP64, the end samples normalised)
+        const double mi = S.mu[i], si = S.isg[i], mj = S.mu[j], sj = S.isg[j];
         double qv[6], tv[6];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -460,11 +524,15 @@ int paa_block(int m) {
   return 8;
 }
 
-void launch_paa_prep(const DevSeries& S, cudaStream_t st) {
+int launch_paa_prep(const DevSeries& S, cudaStream_t st) {
   const int nb = (int)((S.n + (1 << kBlkShift) - 1) >> kBlkShift);
   k_slide_means<<<(unsigned)((S.n + 255) / 256), 256, 0, st>>>(S, S.paa_b);
   k_block_max<<<nb, 256, 0, st>>>(S, nb);
   k_window_scale<<<(unsigned)((S.s + 255) / 256), 256, 0, st>>>(S);
+  if (!S.pq2) return 3;
+  k_block_max2<<<(unsigned)(2 * kCopyBlocks(S.n)), 256, 0, st>>>(S);
+  k_window_rec<<<(unsigned)((S.s + 255) / 256), 256, 0, st>>>(S);
+  return 5;
 }
 
 void launch_paa(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int tile_begin,
