@@ -101,20 +101,24 @@ __host__ __device__ inline GroupLayout group_layout(int m, int w, int C, int G, 
 // q[r] and tw(c) returns t[r + d_lo + c].  With LIVE false the lane keeps its
 // row (a lane that has not reached row 0 yet), and its neighbours read its
 // unchanged cells: for row 0 those are the virtual row -1 (0 on d = 0, +inf
-// elsewhere), exactly what row 0 needs.
-template <typename T, int C, int G, typename TW>
+// elsewhere), exactly what row 0 needs.  HI selects the cells that take the
+// band mask: every cell (HI = -2), none (HI = -1) or cell HI alone (the
+// layouts of dtw_band that keep the lanes past the band huge by their q).
+template <typename T, int C, int G, int HI, typename TW>
 __device__ __forceinline__ void band_step(T qr, const TW& tw, bool live, int g, unsigned int gm,
                                           const T (&pen)[C], T (&A)[C]) {
   // Lane 0's left neighbour and lane G-1's right neighbour wrap around the
   // group, so no lane needs a select: C G is even and 2w + 1 odd, so C G >
   // 2w + 1 and lane G-1's last cell lies past the band; its +inf penalty
-  // keeps it +inf, which is what lane 0's first cell (d = -w) needs on its
-  // left, and makes whatever comes from the right irrelevant to it.
+  // (or its huge cost) keeps it huge, which is what lane 0's first cell
+  // (d = -w) needs on its left, and makes whatever comes from the right
+  // irrelevant to it.
   const T left = __shfl_sync(gm, A[C - 1], (g + G - 1) & (G - 1), G);
   {
     const T d = qr - tw(0);
     const T v = fmin3_(A[1], A[0], left);
-    const T x = fmax_(fma(d, d, v), pen[0]);
+    T x = fma(d, d, v);
+    if (HI == -2 || HI == 0) x = fmax_(x, pen[0]);
     A[0] = live ? x : A[0];
   }
   const T right = __shfl_sync(gm, A[0], (g + 1) & (G - 1), G);
@@ -123,7 +127,8 @@ __device__ __forceinline__ void band_step(T qr, const TW& tw, bool live, int g, 
     const T up = (c + 1 < C) ? A[c + 1 < C ? c + 1 : 0] : right;
     const T d = qr - tw(c);
     const T v = fmin3_(up, A[c], A[c - 1]);
-    const T x = fmax_(fma(d, d, v), pen[c]);
+    T x = fma(d, d, v);
+    if (HI == -2 || HI == c) x = fmax_(x, pen[c]);
     A[c] = live ? x : A[c];
   }
 }
@@ -141,7 +146,18 @@ __device__ __forceinline__ void band_step(T qr, const TW& tw, bool live, int g, 
 // every 16 steps whether every lane's latest row, plus the cumulative bound
 // of the rows still ahead, exceeds the threshold; it then returns +inf and
 // reports the cells it swept.
-template <typename T, int C, int G, bool ABANDON>
+//
+// Band mask: HI = -2 masks every cell past the band.  Otherwise HI is the
+// cell, (2w + 1) mod C, at which diagonal w + 1 (the first past the band)
+// sits in its lane (-1 when that is the lane's first cell), and only that
+// cell is masked: it walls the band off from the diagonals beyond, and the
+// lanes whose cells all lie past the band (after that lane, or from it when
+// HI = -1) read the q sentinel instead of q, so every cell they compute is at
+// least 1e36 with no mask.  Lane 0's left neighbour is then such a cell, the
+// cells between the wall and those lanes only see huge values, and every cell
+// of the band, the abandoning test and the result are the same as with the
+// full mask.
+template <typename T, int C, int G, bool ABANDON, int HI = -2>
 __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, int w,
                       const float* __restrict__ cbc, int nc, float thr,
                       const unsigned int* bsf2, unsigned int gm, int g,
@@ -157,6 +173,9 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
   }
   const T* qg = q - g;         // qg[tau] = q[row]
   const T* tg = t - g + d_lo;  // tg[tau + c] = t[row + d_lo + c]
+  const int g_past = (2 * w + 1) / C + (HI == -1 ? 0 : 1);
+  const bool past = HI != -2 && g >= g_past;  // reads the sentinel q[-1 - x]
+  const T PQ = Pad<T>::q();
   const int g0 = w / C, c0 = w % C;
   const int tau_end = m - 1 + g0;  // lane g0 (cell c0 on d = 0) reaches row m - 1
   *abandoned = false;
@@ -165,7 +184,8 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
   int tau = 0;
   for (; tau < warm; ++tau) {
     const T* tp = tg + tau;
-    band_step<T, C, G>(qg[tau], [tp](int c) { return tp[c]; }, tau - g >= 0, g, gm, pen, A);
+    band_step<T, C, G, HI>(past ? PQ : qg[tau], [tp](int c) { return tp[c]; }, tau - g >= 0, g,
+                           gm, pen, A);
   }
   // blocks of C steps with q and t in registers
   constexpr int kAbEvery = (16 + C - 1) / C;  // blocks between abandon checks
@@ -176,7 +196,8 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
     for (int x = 0; x < C - 1; ++x) W[x] = tg[tau + x];
   }
   const T* tb = tg + tau + C - 1;  // the block's new values of t, and of q,
-  const T* qb = qg + tau;           // at immediate offsets from two pointers
+  const T* qb = past ? q - C : qg + tau;  // at immediate offsets from two pointers
+  const int qstep = past ? 0 : C;
   while (tau + C - 1 <= tau_end) {
     T Qv[C];
 #pragma unroll
@@ -185,10 +206,10 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
       Qv[x] = qb[x];
     }
     tb += C;
-    qb += C;
+    qb += qstep;
 #pragma unroll
     for (int k = 0; k < C; ++k)
-      band_step<T, C, G>(Qv[k], [&W, k](int c) { return W[k + c]; }, true, g, gm, pen, A);
+      band_step<T, C, G, HI>(Qv[k], [&W, k](int c) { return W[k + c]; }, true, g, gm, pen, A);
 #pragma unroll
     for (int x = 0; x < C - 1; ++x) W[x] = W[x + C];
     tau += C;
@@ -224,7 +245,8 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
   // the last steps (fewer than C)
   for (; tau <= tau_end; ++tau) {
     const T* tp = tg + tau;
-    band_step<T, C, G>(qg[tau], [tp](int c) { return tp[c]; }, true, g, gm, pen, A);
+    band_step<T, C, G, HI>(past ? PQ : qg[tau], [tp](int c) { return tp[c]; }, true, g, gm, pen,
+                           A);
   }
   T result = INF;
 #pragma unroll
@@ -237,7 +259,7 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
 
 // The pair consumer: every group takes pairs from the queue until it is
 // drained.  flags bit 0: run the bounds (otherwise DTW only, for seeds).
-template <int C, int G>
+template <int C, int G, int HI>
 __global__ void __launch_bounds__(256) k_pairs(DevSeries S, DevSearch Q, const int2* pairs,
                                                 const unsigned int* npairs, int flags,
                                                 int group_floats) {
@@ -367,7 +389,7 @@ __global__ void __launch_bounds__(256) k_pairs(DevSeries S, DevSearch Q, const i
     unsigned long long cells = 0;
     bool ab = false;
     const float d2 =
-        dtw_band<float, C, G, true>(q, t, m, w, cbc, lay.nc, thr, bsf2, gm, g, &cells, &ab);
+        dtw_band<float, C, G, true, HI>(q, t, m, w, cbc, lay.nc, thr, bsf2, gm, g, &cells, &ab);
     if (g == 0) {
       atomicAdd(&cnt[kDtwCalls], 1ull);
       atomicAdd(&cnt[kDtwCells], cells);
@@ -501,7 +523,7 @@ __global__ void k_best_f32(const Candidate* cands, const unsigned int* count_ptr
 
 // ---- dispatch ----
 
-template <int C, int G>
+template <int C, int G, int HI>
 void run_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
                const unsigned int* npairs, int flags, int num_sms, cudaStream_t st,
                int warps) {
@@ -517,11 +539,44 @@ void run_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
   }
   const int gpb = threads / G;
   bytes = (size_t)gpb * lay.total * sizeof(float);
-  cudaFuncSetAttribute(k_pairs<C, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_pairs<C, G, HI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       200 * 1024);
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs<C, G>, threads, bytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs<C, G, HI>, threads, bytes);
   if (per_sm < 1) per_sm = 1;
-  k_pairs<C, G><<<num_sms * per_sm, threads, bytes, st>>>(S, Q, pairs, npairs, flags, lay.total);
+  k_pairs<C, G, HI><<<num_sms * per_sm, threads, bytes, st>>>(S, Q, pairs, npairs, flags,
+                                                              lay.total);
+}
+
+// The one-pair-per-warp layouts with at most 8 cells per lane run with the
+// single-cell band mask (HI = (2w + 1) mod C, -1 for 0; an even C only sees
+// odd values); the others mask every cell.
+template <int C, int G, int K>
+bool run_pairs_hi(int hi, const DevSeries& S, const DevSearch& Q, const int2* pairs,
+                  const unsigned int* npairs, int flags, int num_sms, cudaStream_t st,
+                  int warps) {
+  if constexpr (K < C) {
+    if constexpr (C % 2 == 1 || K % 2 == 1) {
+      if (hi == K) {
+        run_pairs<C, G, K == 0 ? -1 : K>(S, Q, pairs, npairs, flags, num_sms, st, warps);
+        return true;
+      }
+    }
+    return run_pairs_hi<C, G, K + 1>(hi, S, Q, pairs, npairs, flags, num_sms, st, warps);
+  } else {
+    return false;
+  }
+}
+
+template <int C, int G>
+void run_pairs_band(const DevSeries& S, const DevSearch& Q, const int2* pairs,
+                    const unsigned int* npairs, int flags, int num_sms, cudaStream_t st,
+                    int warps) {
+  if constexpr (G == 32 && C <= 8) {
+    if (run_pairs_hi<C, G, 0>((2 * S.w + 1) % C, S, Q, pairs, npairs, flags, num_sms, st, warps))
+      return;
+  }
+  run_pairs<C, G, -2>(S, Q, pairs, npairs, flags, num_sms, st, warps);
 }
 
 template <typename T, int C, int G>
@@ -634,7 +689,7 @@ void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
   const int flags = bounds ? 1 : 0;
 #define X(c, g) \
   if (band.C == c && band.G == g) {                                               \
-    run_pairs<c, g>(S, Q, pairs, npairs, flags, num_sms, st, band.warps);          \
+    run_pairs_band<c, g>(S, Q, pairs, npairs, flags, num_sms, st, band.warps);     \
     return;                                                                        \
   }
   DTWJ_BAND_CASES(X)
