@@ -142,7 +142,10 @@ __device__ __forceinline__ void band_step(T qr, const TW& tw, bool live, int g, 
 // x < 2C - 1, over a block (its cells of consecutive steps overlap in t), so
 // it loads C values of q and C new values of t per block into registers and
 // keeps the C - 1 values of t the next block shares: two shared-memory loads
-// and two shuffles per step for C cells.  With ABANDON the group checks about
+// and two shuffles per step for C cells.  The blocks run two per loop
+// iteration over a ring of 2C registers of t, so no value is copied between
+// registers and the loop's pointer and counter updates come once per 2C
+// steps.  With ABANDON the group checks about
 // every 16 steps whether every lane's latest row, plus the cumulative bound
 // of the rows still ahead, exceeds the threshold; it then returns +inf and
 // reports the cells it swept.
@@ -187,32 +190,37 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
     band_step<T, C, G, HI>(past ? PQ : qg[tau], [tp](int c) { return tp[c]; }, tau - g >= 0, g,
                            gm, pen, A);
   }
-  // blocks of C steps with q and t in registers
-  constexpr int kAbEvery = (16 + C - 1) / C;  // blocks between abandon checks
+  // blocks of C steps with q and t in registers, two per iteration: W is a
+  // ring of 2C values of t (offset x from the iteration's first step at
+  // W[x mod 2C]), so no value moves between registers
+  constexpr int kAbEvery = (16 + 2 * C - 1) / (2 * C);  // iterations between abandon checks
   int ab_count = kAbEvery;
-  T W[2 * C - 1];  // W[x] = tg[tau + x] at the block's first step tau
+  T W[2 * C];
   if (tau + C - 1 <= tau_end) {
 #pragma unroll
     for (int x = 0; x < C - 1; ++x) W[x] = tg[tau + x];
   }
-  const T* tb = tg + tau + C - 1;  // the block's new values of t, and of q,
-  const T* qb = past ? q - C : qg + tau;  // at immediate offsets from two pointers
-  const int qstep = past ? 0 : C;
-  while (tau + C - 1 <= tau_end) {
-    T Qv[C];
+  const T* tb = tg + tau + C - 1;  // the blocks' new values of t, and of q,
+  const T* qb = past ? q - 2 * C : qg + tau;  // at immediate offsets from two pointers
+  const int qstep = past ? 0 : 2 * C;
+  while (tau + 2 * C - 1 <= tau_end) {
+    T Qv[2 * C];
 #pragma unroll
-    for (int x = 0; x < C; ++x) {
-      W[C - 1 + x] = tb[x];
-      Qv[x] = qb[x];
-    }
-    tb += C;
-    qb += qstep;
+    for (int x = 0; x < C; ++x) W[C - 1 + x] = tb[x];
+#pragma unroll
+    for (int x = 0; x < 2 * C; ++x) Qv[x] = qb[x];
 #pragma unroll
     for (int k = 0; k < C; ++k)
       band_step<T, C, G, HI>(Qv[k], [&W, k](int c) { return W[k + c]; }, true, g, gm, pen, A);
 #pragma unroll
-    for (int x = 0; x < C - 1; ++x) W[x] = W[x + C];
-    tau += C;
+    for (int x = 0; x < C; ++x) W[(2 * C - 1 + x) % (2 * C)] = tb[C + x];
+#pragma unroll
+    for (int k = 0; k < C; ++k)
+      band_step<T, C, G, HI>(Qv[C + k], [&W, k](int c) { return W[(C + k + c) % (2 * C)]; }, true,
+                             g, gm, pen, A);
+    tb += 2 * C;
+    qb += qstep;
+    tau += 2 * C;
     if (ABANDON && --ab_count == 0 && tau <= tau_end) {
       ab_count = kAbEvery;
       const int r = tau - 1 - g;  // this lane's latest row
@@ -241,6 +249,19 @@ __device__ T dtw_band(const T* __restrict__ q, const T* __restrict__ t, int m, i
         return INF;
       }
     }
+  }
+  // one more block when it fits (W holds offsets 0 .. C - 2 of tau)
+  if (tau + C - 1 <= tau_end) {
+    T Qv[C];
+#pragma unroll
+    for (int x = 0; x < C; ++x) {
+      W[C - 1 + x] = tb[x];
+      Qv[x] = qb[x];
+    }
+#pragma unroll
+    for (int k = 0; k < C; ++k)
+      band_step<T, C, G, HI>(Qv[k], [&W, k](int c) { return W[k + c]; }, true, g, gm, pen, A);
+    tau += C;
   }
   // the last steps (fewer than C)
   for (; tau <= tau_end; ++tau) {

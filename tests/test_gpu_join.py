@@ -240,6 +240,25 @@ def test_context_reuse_leaves_no_stale_state(gpu_dtwj, oracle, synth):
             assert 0 <= r.i < r.j < x.size - m + 1
 
 
+def test_band_mask_cell_of_every_residue(gpu_dtwj, synth, oracle):
+    # the join's DTW masks one cell per row step, the one holding diagonal
+    # w + 1 at (2w + 1) mod C, with the lanes past the band on the q
+    # sentinel: every residue of the one-pair-per-warp layouts with up to 8
+    # cells per lane (C = 2 for w < 32, 3 to w = 47, 4 to 63, ... 8 to 127)
+    # must reproduce the oracle's join
+    ws = [5, 31, 32, 33, 34, 52, 53, 64, 65, 66, 67, 68, 80, 81, 82,
+          96, 97, 98, 99, 100, 101, 102, 112, 113, 114, 115]
+    x = synth.random_walk(1500, 7)
+    e = synth.ecg_like(1500, 7)
+    with gpu_dtwj.Context() as ctx:
+        for w in ws:
+            ref = oracle.join(x, 128, w)
+            _check(ctx.join(x, 128, w), ref.i, ref.j, ref.dist, ("rw", w))
+        for w in (31, 33, 34, 53):
+            ref = oracle.join(e, 128, w)
+            _check(ctx.join(e, 128, w), ref.i, ref.j, ref.dist, ("ecg", w))
+
+
 def test_every_band_layout_gives_the_same_join(gpu_dtwj, golden, synth, oracle):
     # the autotuner may pick any layout: each must reproduce the result
     x = synth.random_walk(3500, 6)
