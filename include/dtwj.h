@@ -72,6 +72,11 @@ extern "C" {
                                    runs of the fast bound's survivors, instead of
                                    the default block-mean LB_Keogh bound; the
                                    same result, more pairs reach LB_Keogh      */
+#define DTWJ_F_PETITJEAN 0x100u /* LB_Petitjean (lbPetitjean_new,
+                                   CPU_version1/LB_PETITJEAN.cpp:10-123) on the
+                                   pairs that pass LB_Keogh, before DTW, where
+                                   2 (m + 2 min(w, m - 1)) doubles fit 200 KiB
+                                   (no effect beyond); the same result         */
 
 /* phases reported in dtwj_result.phase_seconds / phase_launches */
 #define DTWJ_PHASE_PREP 0       /* statistics, envelopes, mask, row terms     */
@@ -107,6 +112,7 @@ typedef struct {
   double phase_seconds[8];   /* with DTWJ_F_PROFILE: device time per phase   */
   uint64_t phase_launches[8];/* kernel launches per phase                    */
   uint64_t pruned_paa;     /* pruned by the block-mean LB_Keogh bound (LB_PAA) */
+  uint64_t pruned_petitjean; /* pruned by LB_Petitjean (DTWJ_F_PETITJEAN)    */
 } dtwj_result;
 
 typedef struct dtwj_ctx dtwj_ctx;
@@ -155,6 +161,20 @@ int dtwj_global_mask(const double* x, int64_t n, int32_t m, int32_t w, float* ma
  * device (precise=0) or FP64 (precise=1).  dist[k] for (pi[k], pj[k]). */
 int dtwj_pair_dtw(const double* x, int64_t n, int32_t m, int32_t w, const int64_t* pi,
                   const int64_t* pj, int64_t count, int32_t precise, double* dist);
+
+/* The two sums LB_Petitjean adds to the endpoint bound (lbPetitjean_new,
+ * CPU_version1/LB_PETITJEAN.cpp:10-123, as the join evaluates it at
+ * CPU_version1/new_dtw_motifGUI.cpp:517) for window A = pa[k] against window
+ * B = pb[k], FP64 on the device: keogh_mid[k] = sum over t in [3, m-4] of
+ * (A_t - H_t)^2, H = A projected onto B's envelope; terms[k] = the
+ * projection part.  own_env = 1: each window's own clipped envelope of
+ * radius w (the reference's subs_U / subs_L); 0: the raw series' envelope
+ * normalised per window, as DTWJ_F_PETITJEAN joins read it.  w >= m is taken
+ * as m - 1; DTWJ_ERR_ARG where the shared tables (2 (m + 2w) doubles, plus 4m
+ * with own_env) exceed 200 KiB. */
+int dtwj_pair_lb_petitjean(const double* x, int64_t n, int32_t m, int32_t w, const int64_t* pa,
+                           const int64_t* pb, int64_t count, int32_t own_env, double* keogh_mid,
+                           double* terms);
 
 /* Allocation-free variant of dtwj_pair_dtw for callers that must not allocate
  * device memory (a host framework that reserves the device at start-up, a

@@ -720,3 +720,70 @@ int orc_join(const double* a, int64_t n, int m, int w, unsigned flags, int threa
   free(c.mask); free(c.MN); free(c.MDUL2); free(c.MDUL); free(c.sumE); free(c.SM); free(c.SME);
   return 0;
 }
+
+/* ---- LB_Petitjean (CPU_version1/LB_PETITJEAN.cpp:10-123) ----
+ * The bound adds to LB_Keogh of A against B's envelope a second term for B:
+ * H is A projected onto B's envelope (LB_PETITJEAN.cpp:27-39; the three end
+ * samples of each side keep A's own values, as the reference's copy of q
+ * does at :24), (UH, LH) is H's clipped envelope (:41-88), and each B_k on
+ * k in [3, m-4] adds its distance to [LH_k, UH_k], refined against A's own
+ * envelope where that envelope lies inside (:89-110). */
+static void pj_window(const double* a, int64_t n, int m, int w, int64_t p, int env_mode,
+                      double* z, double* lo, double* up) {
+  double sum = 0.0, ss = 0.0;
+  for (int k = 0; k < m; ++k) sum += a[p + k];
+  const double mu = sum / m;
+  for (int k = 0; k < m; ++k) ss += sq(a[p + k] - mu);
+  const double sg = sqrt(ss / m);
+  for (int k = 0; k < m; ++k) z[k] = (a[p + k] - mu) / sg;
+  if (env_mode) {
+    orc_envelope(z, m, w, lo, up);
+    return;
+  }
+  /* raw envelope of radius w over the series, taken on the slice that holds
+   * every sample the window's envelope reads (clipping at the series ends) */
+  const int64_t b0 = p - w > 0 ? p - w : 0;
+  const int64_t b1 = p + m + w < n ? p + m + w : n;
+  double* sl = (double*)malloc(sizeof(double) * (size_t)(b1 - b0));
+  double* su = (double*)malloc(sizeof(double) * (size_t)(b1 - b0));
+  orc_envelope(a + b0, b1 - b0, w, sl, su);
+  for (int k = 0; k < m; ++k) {
+    lo[k] = (sl[p + k - b0] - mu) / sg;
+    up[k] = (su[p + k - b0] - mu) / sg;
+  }
+  free(sl);
+  free(su);
+}
+
+void orc_lb_petitjean(const double* a, int64_t n, int m, int w, int64_t ia, int64_t ib,
+                      int env_mode, double* keogh_full, double* keogh_mid, double* terms) {
+  if (w > m - 1) w = m - 1;
+  double* buf = (double*)malloc(sizeof(double) * (size_t)m * 9);
+  double *za = buf, *la = buf + m, *ua = buf + 2 * m;
+  double *zb = buf + 3 * m, *lb = buf + 4 * m, *ub = buf + 5 * m;
+  double *h = buf + 6 * m, *lh = buf + 7 * m, *uh = buf + 8 * m;
+  pj_window(a, n, m, w, ia, env_mode, za, la, ua);
+  pj_window(a, n, m, w, ib, env_mode, zb, lb, ub);
+  double km = 0.0;
+  if (keogh_full) *keogh_full = orc_lb_keogh2(za, lb, ub, m);
+  for (int k = 0; k < m; ++k) {
+    h[k] = za[k];
+    if (k >= KIM_BIAS && k < m - KIM_BIAS) {
+      if (za[k] > ub[k]) h[k] = ub[k];
+      else if (za[k] < lb[k]) h[k] = lb[k];
+      km += sq(za[k] - h[k]);
+    }
+  }
+  orc_envelope(h, m, w, lh, uh);
+  double t = 0.0;
+  for (int k = KIM_BIAS; k < m - KIM_BIAS; ++k) {
+    const double x = zb[k];
+    if (x > uh[k] && uh[k] > ua[k]) t += sq(x - ua[k]) - sq(uh[k] - ua[k]);
+    else if (x < lh[k] && lh[k] < la[k]) t += sq(x - la[k]) - sq(lh[k] - la[k]);
+    else if (x > uh[k]) t += sq(x - uh[k]);
+    else if (x < lh[k]) t += sq(x - lh[k]);
+  }
+  *keogh_mid = km;
+  *terms = t;
+  free(buf);
+}

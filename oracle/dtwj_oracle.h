@@ -52,6 +52,18 @@ void orc_kim2(const double* q, const double* t, int m, double* left, double* rig
 int orc_join(const double* a, int64_t n, int m, int w, unsigned flags, int threads,
              orc_result* out);
 double orc_pair_dist(const double* a, int64_t n, int m, int w, int64_t i, int64_t j);
+/* LB_Petitjean of window A = a[ia, ia + m) against window B = a[ib, ib + m)
+ * (lbPetitjean_new, CPU_version1/LB_PETITJEAN.cpp:10-123).  env_mode 1: the
+ * clipped per-window envelopes of the z-normalised windows, as the reference
+ * builds them (subs_U / subs_L, new_dtw_motifGUI.cpp:45); env_mode 0: the
+ * raw series' envelope of radius w, normalised with each window's own
+ * statistics (what the GPU join reads).  w >= m is taken as m - 1.
+ * keogh_full = squared LB_Keogh of A against B's envelope over all m samples
+ * (may be NULL); keogh_mid = the same over k in [3, m-4], i.e. the sum of
+ * (A_k - H_k)^2 with H = A projected onto B's envelope; terms = the
+ * projection part summed over the same k. */
+void orc_lb_petitjean(const double* a, int64_t n, int m, int w, int64_t ia, int64_t ib,
+                      int env_mode, double* keogh_full, double* keogh_mid, double* terms);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,10 @@
 //                                           CPU_version1/compute_shared_data_global.cpp:12,
 //                                           CPU_version1/compute_MASK_global.cpp:10
 //                    with the set-up of new_dtw_motifGUI.cpp:29-45,155-207
+//   ref_lb_petitjean -> LB_KK + lbPetitjean_new
+//                                           CPU_version1/lb_keogh.cpp:9,
+//                                           CPU_version1/LB_PETITJEAN.cpp:10
+//                    on windows set up as new_dtw_motifGUI.cpp:28-46 does
 #include "alldef/matrix.h"
 #include "alldef/allstruct.h"
 #include "allunder/underdtw.h"
@@ -97,6 +101,38 @@ void ref_mvmean(const double* a, long n, int m, double* mu, double* sig) {
   std::vector<double> mv(s), sv(s);
   mvmean(v, m, mv, sv);
   for (long i = 0; i < s; ++i) { mu[i] = mv[i]; sig[i] = sv[i]; }
+}
+
+// LB_Petitjean of window A = a[ia..) against window B = a[ib..) as the
+// reference's join evaluates it (new_dtw_motifGUI.cpp:508-519, with A the
+// window i + diag - 2 and B the window i - 1): the windows z-normalised with
+// mvmean's statistics and each given its clipped envelope by
+// lower_upper_lemire.  keogh = LB_KK of A against B's envelope with no
+// endpoint part and no threshold (the squared LB_Keogh over all m samples);
+// terms = what lbPetitjean_new adds to a zero lbk2 with no threshold.
+void ref_lb_petitjean(const double* a, long n, int m, int w, long ia, long ib,
+                      double* keogh, double* terms) {
+  std::vector<double> v(a, a + n);
+  const long s = n - m + 1;
+  std::vector<double> mu(s), sig(s);
+  mvmean(v, m, mu, sig);
+  std::vector<double> A(m), B(m), la(m), ua(m), lb(m), ub(m);
+  for (int k = 0; k < m; ++k) {
+    A[k] = (a[ia + k] - mu[ia]) / sig[ia];
+    B[k] = (a[ib + k] - mu[ib]) / sig[ib];
+  }
+  lower_upper_lemire(A, m, w, la, ua);
+  lower_upper_lemire(B, m, w, lb, ub);
+  std::vector<double> cb(m, 0.0), proj(m), up(m), lp(m);
+  double sv[2] = {0.0, 0.0};
+  double lbk = 0.0;
+  LB_KK(A, ub.data(), lb.data(), m, 1e300, cb, sv, lbk);
+  *keogh = lbk;
+  double t = 0.0;
+  std::fill(cb.begin(), cb.end(), 0.0);
+  lbPetitjean_new(proj, A, up, lp, ua.data(), la.data(), B, ub.data(), lb.data(), w, m, 1e300,
+                  t, cb, mu[ia], sig[ia]);
+  *terms = t;
 }
 
 void ref_lemire(const double* a, int n, int r, double* lower, double* upper) {

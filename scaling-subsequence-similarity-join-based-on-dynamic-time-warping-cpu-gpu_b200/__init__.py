@@ -44,6 +44,7 @@ F_VERBOSE = 0x10
 F_PROFILE = 0x20
 F_NO_GRAPH = 0x40
 F_MASKED_CASCADE = 0x80
+F_PETITJEAN = 0x100
 
 PHASES = ("prep", "profile", "seeds", "diag", "pairs", "verify", "runs", "keogh")
 
@@ -58,6 +59,7 @@ EXPORTS = (
     "dtwj_matrix_profile",
     "dtwj_global_mask",
     "dtwj_pair_dtw",
+    "dtwj_pair_lb_petitjean",
     "dtwj_pair_dtw_noalloc",
     "dtwj_band",
     "dtwj_strerror",
@@ -119,6 +121,7 @@ class _Result(ctypes.Structure):
         ("phase_seconds", ctypes.c_double * 8),
         ("phase_launches", ctypes.c_uint64 * 8),
         ("pruned_paa", ctypes.c_uint64),
+        ("pruned_petitjean", ctypes.c_uint64),
     ]
 
 
@@ -146,6 +149,7 @@ class JoinResult:
     phase_seconds: list
     phase_launches: list
     pruned_paa: int
+    pruned_petitjean: int = 0
 
     @staticmethod
     def _from(r: _Result) -> "JoinResult":
@@ -181,6 +185,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dtwj_matrix_profile.argtypes = [P(d), i64, i32, P(d), P(i64)]
     lib.dtwj_global_mask.argtypes = [P(d), i64, i32, i32, P(ctypes.c_float), P(i32)]
     lib.dtwj_pair_dtw.argtypes = [P(d), i64, i32, i32, P(i64), P(i64), i64, i32, P(d)]
+    lib.dtwj_pair_lb_petitjean.argtypes = [P(d), i64, i32, i32, P(i64), P(i64), i64, i32, P(d),
+                                           P(d)]
     vp = ctypes.c_void_p
     lib.dtwj_pair_dtw_noalloc.argtypes = [vp, i64, i32, i32, vp, vp, i64, i32, vp, vp]
     lib.dtwj_band.argtypes = [i32, d, i32]
@@ -455,6 +461,26 @@ def pair_dtw(x, m: int, w: int, pi, pj, precise: bool = True) -> np.ndarray:
     return out
 
 
+def pair_lb_petitjean(x, m: int, w: int, pa, pb, own_env: bool = False):
+    """The two sums LB_Petitjean adds to the endpoint bound for windows
+    pa[k] (A) against pb[k] (B): (keogh_mid, terms), FP64 on the device.
+    own_env: each window's own clipped envelope (the reference's); else the
+    raw series' envelope normalised per window (what DTWJ_F_PETITJEAN joins
+    read)."""
+    a = _f64(x)
+    pa = np.ascontiguousarray(pa, dtype=np.int64)
+    pb = np.ascontiguousarray(pb, dtype=np.int64)
+    km = np.empty(pa.size, dtype=np.float64)
+    tt = np.empty(pa.size, dtype=np.float64)
+    P64 = ctypes.POINTER(ctypes.c_int64)
+    rc = load().dtwj_pair_lb_petitjean(_dptr(a), a.size, m, w, pa.ctypes.data_as(P64),
+                                       pb.ctypes.data_as(P64), pa.size, 1 if own_env else 0,
+                                       _dptr(km), _dptr(tt))
+    if rc != OK:
+        raise DtwjError(rc, "dtwj_pair_lb_petitjean")
+    return km, tt
+
+
 def dtw_motif_discovery(ts, subseqlen: int, maxwarp: int, output_time_file_path: str,
                         flags: int = 0, quiet: bool = False) -> JoinResult:
     """Mirror of DTWMotifDiscoveryGUI (CPU_version1/DTWMotifDiscoveryGUI.cpp:12):
@@ -583,7 +609,7 @@ def time_band(m: int, w: int, C: int, G: int, pairs: int = 2048, device: int = 0
 
 
 _COUNTERS = ("pairs", "pruned_fast", "pruned_kim", "pruned_masked", "pruned_paa", "pruned_keogh",
-             "dtw_calls",
+             "pruned_petitjean", "dtw_calls",
              "dtw_abandoned", "dtw_cells", "candidates")
 
 

@@ -23,7 +23,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
-CU_SOURCES = ["prep.cu", "mp.cu", "lb.cu", "runs.cu", "paa.cu", "pairs.cu", "join.cu", "noalloc.cu", "mlp.cu",
+CU_SOURCES = ["prep.cu", "mp.cu", "lb.cu", "runs.cu", "paa.cu", "pairs.cu", "petitjean.cu", "join.cu", "noalloc.cu", "mlp.cu",
               "features.cu", "load.cpp"]
 
 

@@ -122,6 +122,7 @@ enum Counter {
   kDtwCells,
   kCandidates,
   kPrunedPaa,
+  kPrunedPetitjean,
   kNumCounters
 };
 
@@ -333,6 +334,16 @@ int launch_paa_prep(const DevSeries& S, cudaStream_t st);
 // LB_Keogh over the candidates the run filter queued in Q.kq; survivors go to
 // Q.queue.
 void launch_keogh(const DevSeries& S, const DevSearch& Q, int num_sms, cudaStream_t st);
+// LB_Petitjean (csrc/petitjean.cu): the join stage filters the DTW queue of a
+// chunk in place (next: a zeroed work counter); it runs when one warp's
+// shared tables, 2 (m + 2w) doubles, fit kPjMaxSmemBytes.
+constexpr size_t kPjMaxSmemBytes = 200 * 1024;
+bool petitjean_fits(int m, int w);
+void launch_petitjean(const DevSeries& S, const DevSearch& Q, unsigned int* next, int num_sms,
+                      cudaStream_t st);
+size_t lbp_list_bytes(int m, int w, bool own_env);
+void launch_lbp_list(const DevSeries& S, const int2* pairs, int count, bool own_env,
+                     double* keogh_mid, double* terms, int num_sms, cudaStream_t st);
 // bounds = false: DTW only (the seeds); true: endpoint bound + LB_Keogh first
 void launch_pairs(const DevSeries& S, const DevSearch& Q, const int2* pairs,
                   const unsigned int* npairs, bool bounds, BandShape band, int num_sms,

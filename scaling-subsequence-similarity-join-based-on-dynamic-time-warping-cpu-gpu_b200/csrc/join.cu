@@ -402,6 +402,9 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   const bool cascade = (flags & DTWJ_F_MASKED_CASCADE) != 0;
   const bool masked = cascade && !(flags & DTWJ_F_NO_MASKED) && !(flags & DTWJ_F_NO_DIAG);
   const bool verbose = flags & DTWJ_F_VERBOSE;
+  // LB_Petitjean between LB_Keogh and DTW, where its shared tables fit
+  const bool petitjean = (flags & DTWJ_F_PETITJEAN) && !(flags & DTWJ_F_NO_DIAG) &&
+                         petitjean_fits(m, w);
   cudaStream_t st = ctx->stream;
   Phases ph(ctx, (flags & DTWJ_F_PROFILE) != 0);
   CUDA_OK(cudaEventRecord(ctx->ev0, st));
@@ -574,7 +577,8 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
     if (!enumerate_all) {
       ph.begin();
       launch_keogh(S, Q, ctx->num_sms, st);
-      ph.end(DTWJ_PHASE_KEOGH, 1);
+      if (petitjean) launch_petitjean(S, Q, qc + 7, ctx->num_sms, st);
+      ph.end(DTWJ_PHASE_KEOGH, petitjean ? 2 : 1);
     }
     ph.begin();
     launch_pairs(S, Q, Q.queue, Q.queue_count, true, band, ctx->num_sms, st);
@@ -678,7 +682,8 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
         key.insert(key.end(), b, b + bytes);
       };
       const int band_cg[3] = {band.C, band.G, band.warps};
-      const int64_t misc[11] = {nlb, chunk, enumerate_all, masked, cascade, ctx->num_sms, ph.on,
+      const int64_t misc[12] = {nlb, chunk, enumerate_all, masked, cascade, petitjean,
+                                ctx->num_sms, ph.on,
                                 (int64_t)ph.used, (int64_t)(uintptr_t)lbtiles,
                                 (int64_t)(uintptr_t)bits, (int64_t)(uintptr_t)notes};
       put(&S, sizeof S);
@@ -842,6 +847,7 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
       out->pruned_masked = cnt_h[kPrunedMasked];
       out->pruned_keogh = cnt_h[kPrunedKeogh];
       out->pruned_paa = cnt_h[kPrunedPaa];
+      out->pruned_petitjean = cnt_h[kPrunedPetitjean];
       out->dtw_calls = cnt_h[kDtwCalls];
       out->dtw_abandoned = cnt_h[kDtwAbandoned];
       out->dtw_cells = cnt_h[kDtwCells];
@@ -1337,6 +1343,52 @@ int dtwj_pair_dtw(const double* x, int64_t n, int32_t m, int32_t w, const int64_
       break;
     }
     for (int64_t k = 0; k < count; ++k) dist[k] = std::sqrt(dist[k]);
+  } while (0);
+  dtwj_ctx_destroy(ctx);
+  return rc;
+}
+
+int dtwj_pair_lb_petitjean(const double* x, int64_t n, int32_t m, int32_t w, const int64_t* pa,
+                           const int64_t* pb, int64_t count, int32_t own_env, double* keogh_mid,
+                           double* terms) {
+  if (!pa || !pb || !keogh_mid || !terms || count < 0 || count > INT32_MAX) return DTWJ_ERR_ARG;
+  int rc = check_args(x, n, m, w);
+  if (rc) return rc;
+  const int we = effective_band(m, w);
+  if (lbp_list_bytes(m, we, own_env != 0) > kPjMaxSmemBytes) return DTWJ_ERR_ARG;
+  const int64_t s = n - m + 1;
+  std::vector<int2> pairs((size_t)count);
+  for (int64_t k = 0; k < count; ++k) {
+    if (pa[k] < 0 || pb[k] < 0 || pa[k] >= s || pb[k] >= s) return DTWJ_ERR_ARG;
+    pairs[k] = make_int2((int)pa[k], (int)pb[k]);
+  }
+  if (count == 0) return DTWJ_OK;
+  dtwj_ctx* ctx = nullptr;
+  rc = dtwj_ctx_create(0, &ctx);
+  if (rc) return rc;
+  do {
+    double* dev = nullptr;
+    if ((rc = upload(ctx, x, n, &dev))) break;
+    DevSeries S;
+    if ((rc = prepare(ctx, dev, n, m, we, false, nullptr, 1, &S))) break;
+    void* p;
+    if ((rc = ensure(ctx, B_PAIRS, (size_t)count * sizeof(int2), &p))) break;
+    int2* dp = (int2*)p;
+    if ((rc = ensure(ctx, B_OUT, (size_t)count * 16, &p))) break;
+    double* dout = (double*)p;
+    cudaMemcpyAsync(dp, pairs.data(), (size_t)count * sizeof(int2), cudaMemcpyHostToDevice,
+                    ctx->stream);
+    launch_lbp_list(S, dp, (int)count, own_env != 0, dout, dout + count, ctx->num_sms,
+                    ctx->stream);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(keogh_mid, dout, (size_t)count * 8, cudaMemcpyDeviceToHost,
+                        ctx->stream) != cudaSuccess ||
+        cudaMemcpyAsync(terms, dout + count, (size_t)count * 8, cudaMemcpyDeviceToHost,
+                        ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      rc = DTWJ_ERR_CUDA;
+      break;
+    }
   } while (0);
   dtwj_ctx_destroy(ctx);
   return rc;

@@ -108,6 +108,22 @@ class Oracle:
                         mpi.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
         return mp, mpi
 
+    def lb_petitjean(self, x, m, w, a, b, exact_env=True):
+        """(keogh_full, keogh_mid, terms) of window a against window b."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        kf, km, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self.lib.orc_lb_petitjean(self._p(x), ctypes.c_int64(x.size), m, w, ctypes.c_int64(a),
+                                  ctypes.c_int64(b), int(bool(exact_env)), ctypes.byref(kf),
+                                  ctypes.byref(km), ctypes.byref(t))
+        return kf.value, km.value, t.value
+
+    def kim2(self, q, t):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        left, right = ctypes.c_double(), ctypes.c_double()
+        self.lib.orc_kim2(self._p(q), self._p(t), q.size, ctypes.byref(left), ctypes.byref(right))
+        return left.value + right.value
+
     def mask(self, x, m, w):
         x = np.ascontiguousarray(x, dtype=np.float64)
         out = np.empty(x.size)
@@ -137,6 +153,12 @@ def golden():
 @pytest.fixture(scope="session")
 def kat():
     with open(os.path.join(GOLDEN, "kat.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def petitjean_kat():
+    with open(os.path.join(GOLDEN, "petitjean.json")) as f:
         return json.load(f)
 
 

@@ -100,3 +100,42 @@ def test_mask_matches_reference_mask_global(oracle, synth, kat):
         mask, lt = oracle.mask(x, c["m"], c["w"])
         assert lt == c["table_len"]
         assert np.array_equal(np.flatnonzero(mask == 1.0), np.array(c["ones"])), c
+
+
+def _kat_series(synth, rec):
+    gen = synth.random_walk if rec["kind"] == "rw" else synth.ecg_like
+    return np.ascontiguousarray(gen(rec["n"], rec["seed"]), dtype=np.float64)
+
+
+def test_lb_petitjean_matches_reference(oracle, synth, petitjean_kat):
+    """The restated LB_Petitjean (exact per-window envelopes) against the
+    reference's own lbPetitjean_new and LB_KK (tests/golden/petitjean.json):
+    both parts within 1e-9 relative, every record."""
+    checked = 0
+    for rec in petitjean_kat:
+        x = _kat_series(synth, rec)
+        for a, b, keogh, terms in rec["pairs"]:
+            kf, km, t = oracle.lb_petitjean(x, rec["m"], rec["w"], a, b, exact_env=True)
+            assert kf == pytest.approx(keogh, rel=1e-9, abs=1e-12), (rec["m"], rec["w"], a, b)
+            assert t == pytest.approx(terms, rel=1e-9, abs=1e-12), (rec["m"], rec["w"], a, b)
+            assert km <= kf * (1 + 1e-12) + 1e-12
+            checked += 1
+    assert checked > 300
+
+
+def test_lb_petitjean_is_admissible(oracle, synth, petitjean_kat):
+    """endpoint bound + LB_Keogh on [3, m-4] + the projection terms never
+    exceeds the squared DTW, with either envelope (the per-window one the
+    reference builds and the raw-series one the GPU join reads)."""
+    for rec in petitjean_kat:
+        x = _kat_series(synth, rec)
+        m, w = rec["m"], rec["w"]
+        mu, sg = oracle.stats(x, m)
+        for a, b, _, _ in rec["pairs"]:
+            za = (x[a:a + m] - mu[a]) / sg[a]
+            zb = (x[b:b + m] - mu[b]) / sg[b]
+            d2 = oracle.dtw(za, zb, min(w, m - 1)) ** 2
+            kim = oracle.kim2(za, zb)
+            for exact in (True, False):
+                _, km, t = oracle.lb_petitjean(x, m, w, a, b, exact_env=exact)
+                assert kim + km + t <= d2 * (1 + 1e-9) + 1e-9, (m, w, a, b, exact, kim + km + t, d2)
