@@ -329,7 +329,7 @@ def run_ours(args):
     # F_PROFILE records CUDA events around every launch group on the join's
     # stream (no synchronisation), so the timed joins also give the per-phase
     # device times the roofline uses.
-    flags = dtwj.F_PROFILE
+    flags = dtwj.F_PROFILE | (dtwj.F_PETITJEAN if args.petitjean else 0)
     for _ in range(args.warmup):
         ctx.join_device(dptr, n, m, w, flags)
     _barrier(dist)
@@ -464,10 +464,12 @@ def run_ours(args):
         "data": "synthetic (seeded random walk + planted motif)",
         "config": {"workload": args.workload, "n": n, "m": m, "w": w,
                    "pairs_per_join": pairs_total, "l2": "inputs+working set > L2 per join",
-                   "parallelism": "tile shards x%d" % world if world > 1 else "single"},
+                   "parallelism": "tile shards x%d" % world if world > 1 else "single",
+                   "lb_petitjean": bool(args.petitjean)},
         "join_seconds": dev_seconds / args.steps,
         "result": {"i": r0.i, "j": r0.j, "dist": r0.dist},
         "pruned": {"fast": r0.pruned_fast, "paa": r0.pruned_paa, "masked": r0.pruned_masked,
+                   "petitjean": r0.pruned_petitjean,
                    "kim": r0.pruned_kim,
                    "keogh": r0.pruned_keogh, "dtw_calls": r0.dtw_calls,
                    "dtw_abandoned": r0.dtw_abandoned},
@@ -564,6 +566,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--learned-reps", type=int, default=5)
+    ap.add_argument("--petitjean", action="store_true",
+                    help="joins with the LB_Petitjean stage (DTWJ_F_PETITJEAN)")
     ap.add_argument("--batch", type=int, default=0,
                     help="time the batched join of this many series (config 4) instead")
     args = ap.parse_args()
