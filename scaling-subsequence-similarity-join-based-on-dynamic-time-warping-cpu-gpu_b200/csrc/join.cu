@@ -18,6 +18,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -26,6 +27,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace dtwj;
@@ -35,6 +37,8 @@ namespace {
 constexpr unsigned int kCandCap = 1u << 20;
 constexpr unsigned int kQueueCapMax = 1u << 26;
 constexpr int kLbChunkTiles = 1024;
+// (m, w) groups of a batch joined at the same time, one context each.
+constexpr int kBatchWorkers = 4;
 
 struct Buf {
   void* p = nullptr;
@@ -1124,42 +1128,71 @@ int dtwj_join_batch(const double* const* xs, const int64_t* ns, const int32_t* m
   };
   std::stable_sort(order.begin(), order.end(),
                    [&](int32_t a, int32_t b) { return key(a) < key(b); });
-  dtwj_ctx* ctx = nullptr;
-  rc = dtwj_ctx_create(0, &ctx);
-  if (rc) return rc;
-  std::vector<double> cat;
-  std::vector<int64_t> sbeg;
-  std::vector<dtwj_result> res;
-  for (int32_t g0 = 0; g0 < count && rc == DTWJ_OK;) {
+  std::vector<std::pair<int32_t, int32_t>> groups;  // [g0, g1) of order
+  for (int32_t g0 = 0; g0 < count;) {
     int32_t g1 = g0;
     while (g1 < count && key(order[g1]) == key(order[g0])) ++g1;
+    groups.push_back({g0, g1});
+    g0 = g1;
+  }
+  // One group's pass on a context: its series stored back to back, joined
+  // together, each result written to its own slot of outs.
+  auto run_group = [&](dtwj_ctx* ctx, int32_t g0, int32_t g1, std::vector<double>& cat,
+                       std::vector<int64_t>& sbeg, std::vector<dtwj_result>& res) -> int {
     const int nser = g1 - g0;
     sbeg.assign(1, 0);
     for (int32_t q = g0; q < g1; ++q) sbeg.push_back(sbeg.back() + ns[order[q]]);
     const int64_t total = sbeg.back();
-    if (total > (int64_t)INT32_MAX - 4) {
-      rc = DTWJ_ERR_ARG;
-      break;
-    }
+    if (total > (int64_t)INT32_MAX - 4) return DTWJ_ERR_ARG;
     cat.resize((size_t)total);
     for (int32_t q = g0; q < g1; ++q)
       memcpy(cat.data() + sbeg[q - g0], xs[order[q]], (size_t)ns[order[q]] * 8);
     double* dev = nullptr;
     Timer t;
-    rc = upload(ctx, cat.data(), total, &dev);
-    if (rc) break;
+    int grc = upload(ctx, cat.data(), total, &dev);
+    if (grc) return grc;
     res.resize((size_t)nser);
-    rc = run_join(ctx, dev, total, sbeg.data(), nser, ms[order[g0]], ws[order[g0]], flags,
-                  res.data(), 0.0);
-    for (int q = 0; q < nser && rc == DTWJ_OK; ++q) {
+    grc = run_join(ctx, dev, total, sbeg.data(), nser, ms[order[g0]], ws[order[g0]], flags,
+                   res.data(), 0.0);
+    for (int q = 0; q < nser && grc == DTWJ_OK; ++q) {
       res[q].w = ws[order[g0 + q]];
       res[q].seconds_total = t.seconds();
       outs[order[g0 + q]] = res[q];
     }
-    g0 = g1;
+    return grc;
+  };
+  // Groups run concurrently, up to kBatchWorkers at a time: each worker
+  // thread owns a context (its own stream and buffers) and takes the next
+  // group until none is left, so one group's host checks and small launches
+  // overlap another's kernels.
+  const int workers = (int)groups.size() < kBatchWorkers ? (int)groups.size() : kBatchWorkers;
+  std::atomic<int> next_group{0};
+  std::atomic<int> first_error{DTWJ_OK};
+  auto worker = [&]() {
+    dtwj_ctx* ctx = nullptr;
+    int wrc = dtwj_ctx_create(0, &ctx);
+    std::vector<double> cat;
+    std::vector<int64_t> sbeg;
+    std::vector<dtwj_result> res;
+    while (wrc == DTWJ_OK && first_error.load() == DTWJ_OK) {
+      const int gi = next_group.fetch_add(1);
+      if (gi >= (int)groups.size()) break;
+      wrc = run_group(ctx, groups[gi].first, groups[gi].second, cat, sbeg, res);
+    }
+    if (wrc != DTWJ_OK) {
+      int expected = DTWJ_OK;
+      first_error.compare_exchange_strong(expected, wrc);
+    }
+    dtwj_ctx_destroy(ctx);
+  };
+  if (workers <= 1) {
+    worker();
+  } else {
+    std::vector<std::thread> pool;
+    for (int k = 0; k < workers; ++k) pool.emplace_back(worker);
+    for (auto& th : pool) th.join();
   }
-  dtwj_ctx_destroy(ctx);
-  return rc;
+  return first_error.load();
 }
 
 int dtwj_matrix_profile(const double* x, int64_t n, int32_t m, double* mp, int64_t* mpi) {

@@ -26,6 +26,22 @@ def test_batch_matches_single_joins(gpu_dtwj, synth):
         assert rb[k].n == len(x) and rb[k].m == m and rb[k].w == w
 
 
+def test_batch_with_more_groups_than_workers(gpu_dtwj, synth):
+    # seven (m, w) groups: the groups run on up to four contexts at a time,
+    # each worker taking the next group when its last one is done
+    shapes = [(32, 2), (48, 3), (64, 4), (64, 13), (96, 5), (128, 7), (160, 8)]
+    xs, ms, ws = [], [], []
+    for k, (m, w) in enumerate(shapes):
+        for r in range(3):
+            gen = synth.random_walk if (k + r) % 2 == 0 else synth.ecg_like
+            xs.append(gen(2500 + 700 * r + 100 * k, 40 + 3 * k + r))
+            ms.append(m)
+            ws.append(w)
+    rb = gpu_dtwj.join_batch(xs, ms, ws)
+    for k, (x, m, w) in enumerate(zip(xs, ms, ws)):
+        _same(rb[k], gpu_dtwj.join(x, m, w), "series %d (n=%d m=%d w=%d)" % (k, len(x), m, w))
+
+
 def test_batch_edge_series(gpu_dtwj, synth):
     # a flat series (no valid window), an exact duplicate (tie at distance 0,
     # lowest index wins) and the shortest allowed length, mixed with plain ones
