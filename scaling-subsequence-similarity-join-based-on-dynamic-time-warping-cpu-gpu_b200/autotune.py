@@ -100,11 +100,12 @@ def apply_entry(ctx, m: int, w: int, e: dict):
 
 
 def tune_join(series, m: int, w: int, cache_path: str | None = None, device: int = 0,
-              warps=(2, 4, 8), chunks=(256, 1024, 2048), measure=None, shapes=None) -> dict:
+              warps=(2, 4, 8), chunks=(0, 256, 1024, 2048), measure=None, shapes=None) -> dict:
     """Tunes a join of (m, w) on a sample series (a prefix of the series to be
     joined, or one like it): first the DTW band layout, then the DTW kernel's
     CTA size in warps, then the sweep's tiles per chunk, each by the device
-    time of a join of the sample with the others at their best so far.  The
+    time of a join of the sample with the others at their best so far (chunk 0
+    is the library's default, four tiles per resident CTA of the sweep).  The
     entry is cached under join_key(m, w); a Context created with this cache
     (tune_cache=, or DTWJ_TUNE_CACHE) applies it before its first join of
     (m, w).  measure(C, G, warps, chunk) -> seconds defaults to a warm-up join

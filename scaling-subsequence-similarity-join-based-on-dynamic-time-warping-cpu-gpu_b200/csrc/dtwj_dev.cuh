@@ -97,6 +97,8 @@ constexpr int kLbPerThread = 7;
 constexpr int kLbLags = kLbThreads * kLbPerThread;
 constexpr int kLbRows = 18 * kLbPerThread * 32;
 constexpr int kLbWords = kLbRows / 32;
+// CTAs of the persistent diagonal sweep per SM (launch bounds of k_lb).
+constexpr int kLbCtasPerSm = 3;
 // Lags per group of the block-mean filter's work items (one lag per lane).
 constexpr int kLbGroups = kLbLags / 32;
 static_assert(kLbLags % 32 == 0, "lag groups of one warp");

@@ -36,7 +36,14 @@ namespace {
 
 constexpr unsigned int kCandCap = 1u << 20;
 constexpr unsigned int kQueueCapMax = 1u << 26;
-constexpr int kLbChunkTiles = 1024;
+// Default tiles per chunk of the sweep: kLbChunkRounds tiles for each of the
+// diagonal sweep's resident CTAs.  Its tiles take about the same time, so a
+// chunk that is not a whole number of rounds leaves CTAs idle in its last
+// round (1024 tiles on 444 CTAs: 2.3 rounds, the last one 31 % busy).  On
+// the 1M-sample bench series 4 rounds (1776 tiles) measured best: 0.973 s
+// per join against 0.998 s at 3 rounds, 0.980 s at 5, 0.985 s at 6 and
+// 1.008 s at 1024 tiles.
+constexpr int kLbChunkRounds = 4;
 // (m, w) groups of a batch joined at the same time, one context each.
 constexpr int kBatchWorkers = 4;
 
@@ -566,7 +573,8 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
   // ---- diagonal sweep in chunks of LB tiles ----
   const bool enumerate_all = flags & DTWJ_F_NO_DIAG;
   const double tile_pairs = (double)kLbLags * kLbRows;
-  int chunk = ctx->chunk_tiles > 0 ? ctx->chunk_tiles : kLbChunkTiles;
+  int chunk = ctx->chunk_tiles > 0 ? ctx->chunk_tiles
+                                   : kLbChunkRounds * kLbCtasPerSm * ctx->num_sms;
   if (enumerate_all) chunk = (int)((double)qcap / tile_pairs) > 0 ? (int)((double)qcap / tile_pairs) : 1;
   unsigned int* bits;
   ENSURE(B_BITS, (size_t)(chunk < nlb ? chunk : (nlb > 0 ? nlb : 1)) * kLbLags * kLbWords * 4, bits);

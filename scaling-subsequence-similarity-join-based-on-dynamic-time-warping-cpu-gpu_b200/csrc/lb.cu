@@ -211,7 +211,7 @@ __device__ __forceinline__ void lb_tile(const DevSeries& S, const DevSearch& Q, 
 
 // Persistent sweep: each CTA takes tiles from the work counter *next until
 // the chunk is exhausted; tile k of the chunk writes its bits to slot k.
-__global__ void __launch_bounds__(kLbThreads, 3) k_lb(DevSeries S, DevSearch Q,
+__global__ void __launch_bounds__(kLbThreads, kLbCtasPerSm) k_lb(DevSeries S, DevSearch Q,
                                                       const Tile* tiles, int ntiles,
                                                       unsigned int* bits, bool enumerate_all,
                                                       unsigned int* next) {
@@ -250,7 +250,7 @@ void launch_lb(const DevSeries& S, const DevSearch& Q, const Tile* tiles, int ti
   if (tile_end <= tile_begin) return;
   cudaFuncSetAttribute(k_lb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LbShared));
   const int ntiles = tile_end - tile_begin;
-  const int resident = 3 * num_sms;  // three CTAs per SM (launch bounds, 64.5 KB shared each)
+  const int resident = kLbCtasPerSm * num_sms;  // launch bounds, 64.5 KB shared each
   k_lb<<<ntiles < resident ? ntiles : resident, kLbThreads, sizeof(LbShared), st>>>(
       S, Q, tiles + tile_begin, ntiles, bits, enumerate_all, next);
 }

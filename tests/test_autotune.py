@@ -62,7 +62,9 @@ def test_tune_join_searches_each_knob_and_caches(tmp_path):
     shapes = lambda w: [(2, 32), (4, 16), (7, 4)]
     e = at.tune_join(None, 256, 13, path, measure=measure, shapes=shapes)
     assert (e["C"], e["G"], e["dtw_warps"], e["chunk_tiles"]) == (2, 32, 8, 256)
-    assert len(calls) == 3 + 3 + 3 and len(e["tried"]) == 9
+    # three layouts, three CTA sizes, four chunk sizes (the default among them)
+    assert len(calls) == 3 + 3 + 4 and len(e["tried"]) == 10
+    assert [c[3] for c in calls[-4:]] == [0, 256, 1024, 2048]
     saved = json.load(open(path))
     assert saved[at.join_key(256, 13)]["dtw_warps"] == 8
     calls.clear()
