@@ -23,7 +23,11 @@
 //   --data2=PATH                second file for --format=first-column
 //   --binary                    same as --format=binary
 //   --json=PATH                 also write the full result as JSON
-//   --no-masked, --no-seed      disable the masked bound / ED seeding
+//   --masked-cascade            the reference's masked diagonal bound and
+//                               endpoint bound as the run filter
+//   --petitjean                 LB_Petitjean between LB_Keogh and DTW
+//   --no-masked, --no-seed      disable the masked bound (with
+//                               --masked-cascade) / ED seeding
 //   --verbose                   phase timings on stderr
 #include "../../include/dtwj.h"
 
@@ -39,7 +43,8 @@ int main(int argc, char** argv) {
     fprintf(stderr,
             "usage: %s <data_path> <time_out_path> <m> <ratio> [--band-rounding=ceil|round]"
             " [--band=W] [--format=values|every|first-column|rows|binary] [--every=N]"
-            " [--data2=PATH] [--binary] [--json=PATH] [--no-masked] [--no-seed] [--verbose]\n",
+            " [--data2=PATH] [--binary] [--json=PATH] [--masked-cascade] [--petitjean]"
+            " [--no-masked] [--no-seed] [--verbose]\n",
             argv[0]);
     return 2;
   }
@@ -64,6 +69,8 @@ int main(int argc, char** argv) {
     else if (!strncmp(a, "--every=", 8)) every = atoi(a + 8);
     else if (!strncmp(a, "--data2=", 8)) data2 = a + 8;
     else if (!strncmp(a, "--json=", 7)) json = a + 7;
+    else if (!strcmp(a, "--masked-cascade")) flags |= DTWJ_F_MASKED_CASCADE;
+    else if (!strcmp(a, "--petitjean")) flags |= DTWJ_F_PETITJEAN;
     else if (!strcmp(a, "--no-masked")) flags |= DTWJ_F_NO_MASKED;
     else if (!strcmp(a, "--no-seed")) flags |= DTWJ_F_NO_SEED;
     else if (!strcmp(a, "--verbose")) flags |= DTWJ_F_VERBOSE;
