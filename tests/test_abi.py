@@ -67,6 +67,31 @@ def test_cli_unopenable_file_mirrors_reference(tmp_path):
     assert "Error opening file" in r.stderr
     r = subprocess.run([cli], capture_output=True, text=True)
     assert r.returncode == 2
+    # every documented option is accepted (parsed before the file is read);
+    # an unknown one is refused
+    for opt in ("--masked-cascade", "--petitjean", "--no-masked", "--no-seed", "--verbose",
+                "--band-rounding=round", "--band=7", "--format=rows", "--json=" + str(tmp_path / "r.json")):
+        r = subprocess.run([cli, str(tmp_path / "missing.txt"), str(tmp_path / "t.txt"), "64",
+                            "0.05", opt], capture_output=True, text=True)
+        assert r.returncode == 0 and "Error opening file" in r.stderr, opt
+    r = subprocess.run([cli, str(tmp_path / "missing.txt"), str(tmp_path / "t.txt"), "64", "0.05",
+                        "--no-such-option"], capture_output=True, text=True)
+    assert r.returncode == 2 and "unknown option" in r.stderr
+
+
+def test_lb_petitjean_argument_errors_before_device_work(dtwj):
+    x = np.random.default_rng(1).standard_normal(3000).cumsum()
+    s = 3000 - 64 + 1
+    for m, w, a, b in [(64, 3, [0], [s]), (64, 3, [-1], [10]), (4, 3, [0], [10]),
+                       (64, -1, [0], [100])]:
+        with pytest.raises(dtwj.DtwjError) as e:
+            dtwj.pair_lb_petitjean(x, m, w, a, b)
+        assert e.value.code == dtwj.ERR_ARG, (m, w, a, b)
+    # tables beyond the shared-memory limit: 2 (m + 2w) + 4m doubles > 200 KiB
+    big = np.random.default_rng(2).standard_normal(40000).cumsum()
+    with pytest.raises(dtwj.DtwjError) as e:
+        dtwj.pair_lb_petitjean(big, 4200, 255, [0], [8400], own_env=True)
+    assert e.value.code == dtwj.ERR_ARG
 
 
 def test_synthetic_generators_are_deterministic(synth):
