@@ -122,8 +122,11 @@ int dtwj_join(const double* x, int64_t n, int32_t m, int32_t w, uint32_t flags,
               dtwj_result* out);
 
 /* Many independent series, each with its own m and w; outs[k] is identical to
- * dtwj_join(xs[k], ns[k], ms[k], ws[k], flags).  No reference counterpart
- * (the reference joins one series per process). */
+ * dtwj_join(xs[k], ns[k], ms[k], ws[k], flags).  Series of one (m, w) are
+ * joined together in one pass; up to four such groups run at the same time,
+ * each on its own host thread and device context (about 4 GB of device
+ * buffers each), all on device 0.  No reference counterpart (the reference
+ * joins one series per process). */
 int dtwj_join_batch(const double* const* xs, const int64_t* ns, const int32_t* ms,
                     const int32_t* ws, int32_t count, uint32_t flags, dtwj_result* outs);
 
