@@ -1193,13 +1193,16 @@ int dtwj_join_batch(const double* const* xs, const int64_t* ns, const int32_t* m
     }
     dtwj_ctx_destroy(ctx);
   };
-  if (workers <= 1) {
-    worker();
-  } else {
-    std::vector<std::thread> pool;
-    for (int k = 0; k < workers; ++k) pool.emplace_back(worker);
-    for (auto& th : pool) th.join();
+  std::vector<std::thread> pool;
+  if (workers > 1) {
+    try {
+      for (int k = 0; k < workers; ++k) pool.emplace_back(worker);
+    } catch (...) {
+      // no more threads: the workers already started take every group
+    }
   }
+  if (pool.empty()) worker();
+  for (auto& th : pool) th.join();
   return first_error.load();
 }
 
