@@ -44,6 +44,11 @@ constexpr unsigned int kQueueCapMax = 1u << 26;
 // per join against 0.998 s at 3 rounds, 0.980 s at 5, 0.985 s at 6 and
 // 1.008 s at 1024 tiles.
 constexpr int kLbChunkRounds = 4;
+// Largest piece an overflowing chunk is swept again in.  Every piece that
+// overflows again wastes a full DTW queue of work, and on the 262,144-sample
+// ECG-like series (w = 103), where nearly every pair reaches LB_Keogh, 32
+// tiles fit the queues where 55 would not.
+constexpr int kResweepTiles = 32;
 // (m, w) groups of a batch joined at the same time, one context each.
 constexpr int kBatchWorkers = 4;
 
@@ -774,7 +779,9 @@ int run_join(dtwj_ctx* ctx, const double* x_dev, int64_t n, const int64_t* sbeg,
         drop[k] += nh[c + 1].counters[k] - nh[c].counters[k];
       const int t0 = ranges[c].first, t1 = ranges[c].second;
       if (t1 - t0 == 1 || attempt >= 4) return DTWJ_ERR_OVERFLOW;
-      const int sub = (t1 - t0) / 32 > 0 ? (t1 - t0) / 32 : 1;
+      int sub = (t1 - t0) / 32;
+      if (sub > kResweepTiles) sub = kResweepTiles;
+      if (sub < 1) sub = 1;
       for (int u = t0; u < t1; u += sub) again.push_back({u, u + sub < t1 ? u + sub : t1});
     }
     if (again.empty()) break;
