@@ -130,6 +130,22 @@ def sweep_tiles(n: int, m: int):
     return ntiles, rows_sum
 
 
+def launch_traffic(tfile: str, kname: str, tiles_per_launch: float):
+    """DRAM bytes per launch of a sweep kernel: the ncu capture of one launch
+    over a full chunk (profiles/ncu_traffic_rw1m_motif.json, its "tiles"
+    field), scaled to this run's average tiles per launch, since each tile
+    moves the same bytes.  None without a capture."""
+    if not os.path.exists(tfile):
+        return None
+    with open(tfile) as f:
+        rec = json.load(f)
+    b = rec.get("bytes_per_launch", {}).get(kname)
+    tiles = rec.get("tiles")
+    if b is None or not tiles:
+        return None
+    return b * tiles_per_launch / tiles
+
+
 def _dist_init():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -428,10 +444,9 @@ def run_ours(args):
     per_launch_s = phases[roof_phase] / nl
     achieved_gbs = alg_bytes / max(phases[roof_phase], 1e-12) / 1e9
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "ncu_traffic_rw1m_motif.json")
-    if os.path.exists(tfile) and args.workload == "rw1m_motif":
-        with open(tfile) as f:
-            traffic = json.load(f).get("bytes_per_launch", {}).get(kname)
+    if args.workload == "rw1m_motif" and kname in ("k_lb", "k_paa"):
+        traffic = launch_traffic(os.path.join(ROOT, "profiles", "ncu_traffic_rw1m_motif.json"),
+                                 kname, ntiles / nl)
     fp64_flops = pairs_total * 12.0  # k_lb: 2 recurrences x 2 DFMA + 2 DFMA tests per pair
     fp64_peak = 148 * 64 * 2 * sm_max * 1e6 / 1e12
     cells_per_s = r0.dtw_cells / max(phases.get("pairs", 1e-12) + phases.get("seeds", 0), 1e-12)
