@@ -45,9 +45,10 @@ constexpr unsigned int kQueueCapMax = 1u << 26;
 // 1.008 s at 1024 tiles.
 constexpr int kLbChunkRounds = 4;
 // Largest piece an overflowing chunk is swept again in.  Every piece that
-// overflows again wastes a full DTW queue of work, and on the 262,144-sample
-// ECG-like series (w = 103), where nearly every pair reaches LB_Keogh, 32
-// tiles fit the queues where 55 would not.
+// overflows again wastes a full DTW queue of work.  On the 262,144-sample
+// ECG-like series at w = 103 nearly every pair reaches LB_Keogh, about 3.5
+// million per tile by that join's stage counts, so 32 tiles fit the LB_Keogh
+// queue (2^27 entries) and 55 would not.
 constexpr int kResweepTiles = 32;
 // (m, w) groups of a batch joined at the same time, one context each.
 constexpr int kBatchWorkers = 4;
