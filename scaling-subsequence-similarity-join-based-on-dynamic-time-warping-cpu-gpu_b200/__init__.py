@@ -250,6 +250,9 @@ def join(x, m: int, w: int, flags: int = 0) -> JoinResult:
 
 
 def join_batch(series, ms, ws, flags: int = 0) -> list[JoinResult]:
+    """Top-1 pair of each series (dtwj_join_batch): the series of one (m, w)
+    are joined together in one pass, up to four such groups at the same time
+    on device 0; each result equals join(series[k], ms[k], ws[k], flags)."""
     arrs = [_f64(x) for x in series]
     k = len(arrs)
     ptrs = (ctypes.POINTER(ctypes.c_double) * k)(*[_dptr(a) for a in arrs])
